@@ -1,0 +1,185 @@
+/* libquasi_gpu: the quasi-incompressible smectic-isotropic pseudo-spectral
+ * time step of evitral/smaiso-quasi on one NVIDIA B200 (sm_100a).
+ *
+ * The reference has no library interface: its step lives inside main() of
+ * quasi/quasi.cpp (and quasi/quasi-stb.cpp) behind FFTW-MPI's plan/execute
+ * calls.  Each entry point below names the reference code it replaces.
+ *
+ * Conventions
+ *   - Every function returns 0 on success and a negative QUASI_ERR_* code on
+ *     failure; quasi_last_error() returns a message for the calling thread.
+ *   - Host arrays use the reference layout a[(i*ny + j)*nz + k] (z fastest,
+ *     x the reference's MPI slab axis), doubles, nx*ny*nz elements.
+ *   - The library owns all device memory of a handle.  A handle is
+ *     single-threaded and issues its work on its own CUDA stream.
+ */
+#ifndef QUASI_GPU_H_
+#define QUASI_GPU_H_
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QUASI_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define QUASI_API __attribute__((visibility("default")))
+#else
+#define QUASI_API
+#endif
+
+enum quasi_status {
+  QUASI_OK = 0,
+  QUASI_ERR_INVALID = -1,    /* bad argument or configuration */
+  QUASI_ERR_CUDA = -2,       /* a CUDA call failed */
+  QUASI_ERR_NOMEM = -3,      /* device or host allocation failed */
+  QUASI_ERR_STATE = -4,      /* call out of order (e.g. step before init) */
+  QUASI_ERR_IO = -5,         /* checkpoint file missing, short or corrupt */
+  QUASI_ERR_NODEVICE = -6,   /* no usable CUDA device */
+  QUASI_ERR_UNSUPPORTED = -7 /* valid request this build does not implement */
+};
+
+enum quasi_variant {
+  QUASI_VARIANT_QUASI = 0, /* quasi/quasi.cpp: density-varying model */
+  QUASI_VARIANT_STB = 1    /* quasi/quasi-stb.cpp: pure smectic, Crank-Nicolson */
+};
+
+enum quasi_precision {
+  QUASI_PREC_FP64 = 0, /* plain form: every field and transform in double */
+  QUASI_PREC_FP32 = 1  /* fields and transforms in float; constants, the
+                          semi-implicit update and reductions in double */
+};
+
+enum quasi_field {
+  QUASI_FIELD_PSI = 0,      /* psi_local          */
+  QUASI_FIELD_RHO = 1,      /* rho_local          */
+  QUASI_FIELD_VX = 2,       /* velx_local         */
+  QUASI_FIELD_VY = 3,       /* vely_local         */
+  QUASI_FIELD_VZ = 4,       /* velz_local         */
+  QUASI_FIELD_P = 5,        /* p_local            */
+  QUASI_FIELD_DIVV = 6,     /* divv_local         */
+  QUASI_FIELD_PSIQ = 7,     /* psiq_local (scaled spectral psi) */
+  QUASI_FIELD_PSIQ_OLD = 8, /* psiq_old_local     */
+  QUASI_FIELD_DTPSI = 9,    /* dtpsi_local (quasi-stb only) */
+  QUASI_FIELD_DF = 10,      /* dfDlapPsi_local    */
+  QUASI_FIELD_COUNT = 11
+};
+
+/* Model and run configuration.  quasi_config_default() fills the reference's
+ * compile-time constants (quasi.cpp:155-219 / quasi-stb.cpp:149-220). */
+typedef struct quasi_config {
+  int nx, ny, nz;       /* grid; each 2^a 3^b in {8..512}, nz % 16 == 0  */
+  int variant;          /* enum quasi_variant                            */
+  int precision;        /* enum quasi_precision                          */
+  int emulate_ranks;    /* reproduce an MPI run of this many ranks (1 or
+                           even, dividing nx): quasi.cpp:1641-1690 reads the
+                           previous rank's first x plane at rank boundaries */
+  int device;           /* CUDA device ordinal                           */
+  double nu_arg;        /* argv[1]: nu (quasi) or nu/0.1 (quasi-stb)     */
+  double ep_arg;        /* argv[2]: epsilon = -0.001 * ep_arg            */
+  double gamma, beta, alpha, q0;
+  double amp;           /* Amp: enters rho_s = kp*Amp + rho_0            */
+  double rho_0, kp;
+  double rho_m;         /* <= 0: rho_s / 2 (quasi.cpp:198)               */
+  double dt;
+  int nw;               /* points per wavelength: dx = 2 pi / (q0 nw)    */
+  int divv_switch;      /* divv on after this step, p coupling one later */
+  double q_pert;        /* quasi-stb growth-rate probe wavenumber Q       */
+} quasi_config;
+
+typedef struct quasi_handle quasi_handle;
+
+QUASI_API int quasi_abi_version(void);
+QUASI_API const char* quasi_last_error(void);
+
+/* Fill `cfg` with the reference defaults of `variant` on an nx*ny*nz grid. */
+QUASI_API int quasi_config_default(quasi_config* cfg, int variant, int nx, int ny, int nz);
+
+/* Allocate device state.  Replaces quasi.cpp:228-495 (MPI init, slab
+ * decomposition, 39 field vectors, 8 fftw_mpi_plan_r2r_3d plans). */
+QUASI_API int quasi_create(const quasi_config* cfg, quasi_handle** out);
+QUASI_API int quasi_destroy(quasi_handle* h);
+
+/* Initial psi from host memory (the reference fills psi_local at
+ * quasi.cpp:506-589 or reads it at quasi.cpp:692-717). */
+QUASI_API int quasi_set_psi(quasi_handle* h, const double* host_psi);
+
+/* Pre-loop projection and first nonlinear term, quasi.cpp:875-951. */
+QUASI_API int quasi_init(quasi_handle* h);
+
+/* Advance nsteps steps (the body of the while loop, quasi.cpp:1014-1965);
+ * the step is one CUDA graph.  Returns when the steps have completed. */
+QUASI_API int quasi_step(quasi_handle* h, int nsteps);
+
+/* As quasi_step, timing the steps with CUDA events on the handle's stream;
+ * *device_ms receives the elapsed device time of the nsteps steps. */
+QUASI_API int quasi_step_timed(quasi_handle* h, int nsteps, double* device_ms);
+
+/* Steps taken since quasi_init (the reference's nLoop). */
+QUASI_API int quasi_step_count(const quasi_handle* h, long* nloop);
+
+/* Copy one field to host memory (doubles, reference layout). */
+QUASI_API int quasi_get_field(quasi_handle* h, int field, double* host_out);
+
+/* L1 = sum|psi - psi_old| / (dt sum|psi|), mass = sum(rho) dx^3,
+ * energy = sum rho(-ep psi^2/2 + alpha df^2/2 - beta psi^4/4 + gamma psi^6/6) dx^3,
+ * accumulated in double: quasi.cpp:1969-2033.  out[2] is 0 for quasi-stb. */
+QUASI_API int quasi_diagnostics(quasi_handle* h, double out[3]);
+
+/* quasi-stb growth rate (psiq - psiq_old)/(dt psiq_old) at the mode
+ * (round(Q/Vqz[1]), 0, round(q0/Vqz[1])): quasi-stb.cpp:2149-2157. */
+QUASI_API int quasi_growth_rate(quasi_handle* h, double* out);
+
+/* Exact binary checkpoint of the carried state (psiq, psiq_old, Nq_old,
+ * rhoq, rho_old, v, divv, psi, nLoop).  The reference restarts from psi text
+ * only (quasi.cpp:692-717); quasi_set_psi + quasi_init reproduce that. */
+QUASI_API int quasi_save(quasi_handle* h, const char* path);
+QUASI_API int quasi_load(quasi_handle* h, const char* path);
+
+/* ---- seeded initial conditions (host only, no device needed) -----------
+ * The reference builds a focal-conic domain (quasi.cpp:543-589) or reads psi
+ * from text (quasi.cpp:692-717); the workloads add planar, undulated,
+ * displaced-interface and droplet smectic-isotropic interfaces. */
+enum quasi_ic_kind {
+  QUASI_IC_PLANAR = 0,     /* A(z) cos(q0 z), A = A0/2 (1 - tanh((z - Lz/2)/w)) */
+  QUASI_IC_UNDULATED = 1,  /* A(z) cos(q0 z + delta sin(2pi x/Lx) sin(2pi y/Ly)) */
+  QUASI_IC_INTERFACE = 2,  /* A(z-h) cos(q0 (z-h)), h = eps_h cos(q_h x)        */
+  QUASI_IC_DROPLET = 3,    /* A(r) cos(q0 z), tanh radial envelope, R = radius_frac L */
+  QUASI_IC_STB = 4,        /* quasi-stb.cpp:549-550 undulated layers           */
+  QUASI_IC_FOCAL_CONIC = 5 /* quasi.cpp:543-589, size aE = bE = fc_size        */
+};
+typedef struct quasi_ic {
+  int kind;
+  unsigned long long seed; /* splitmix64 stream seed for the noise           */
+  double noise;            /* uniform noise amplitude on psi                 */
+  double delta;            /* undulation amplitude                           */
+  double eps_h, q_h;       /* interface displacement                         */
+  double radius_frac;      /* droplet radius / box length                    */
+  double width_wavelengths;/* tanh envelope width w in wavelengths 2 pi/q0   */
+  double amp0;             /* <= 0: A0 = sqrt(9 beta / (10 gamma))            */
+  double fc_size;          /* focal-conic aE = bE (argv[3])                  */
+} quasi_ic;
+QUASI_API int quasi_ic_default(quasi_ic* ic, int kind);
+QUASI_API int quasi_initial_condition(const quasi_config* cfg, const quasi_ic* ic, double* host_psi);
+
+/* ---- lower interface: one 3-D r2r transform with FFTW semantics ---------
+ * kind[a] per axis (x, y, z): 0 REDFT10, 1 REDFT01, 2 RODFT10, 3 RODFT01,
+ * unnormalised, in place.  Replaces fftw_mpi_plan_r2r_3d / fftw_execute
+ * (quasi.cpp:449-495 and every fftw_execute of the loop). */
+typedef struct quasi_r2r_plan quasi_r2r_plan;
+QUASI_API int quasi_r2r_plan_create(int nx, int ny, int nz, const int kind[3], int precision, int device,
+                          quasi_r2r_plan** out);
+/* data: device pointer to nx*ny*nz elements (double for FP64, float for
+ * FP32); stream: a cudaStream_t or NULL for the plan's own stream. */
+QUASI_API int quasi_r2r_execute_device(quasi_r2r_plan* p, void* data, void* stream);
+/* host doubles in -> host doubles out (may alias); copies included. */
+QUASI_API int quasi_r2r_execute_host(quasi_r2r_plan* p, const double* in, double* out);
+QUASI_API int quasi_r2r_plan_destroy(quasi_r2r_plan* p);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QUASI_GPU_H_ */

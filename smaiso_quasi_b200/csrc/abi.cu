@@ -1,0 +1,177 @@
+// The extern "C" boundary declared in include/quasi_gpu.h.
+#include <cuda_runtime.h>
+
+#include <new>
+#include <string>
+
+#include "engine.cuh"
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+bool is_axis_len(int n) {
+  switch (n) {
+    case 8: case 16: case 32: case 64: case 96: case 128: case 192: case 256: case 512: return true;
+    default: return false;
+  }
+}
+
+int device_check(int device) {
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    return fail(QUASI_ERR_NODEVICE, "no CUDA device available (libquasi_gpu has no CPU fallback)");
+  }
+  if (device < 0 || device >= count) return fail(QUASI_ERR_INVALID, "device ordinal out of range");
+  return QUASI_OK;
+}
+
+}  // namespace
+
+namespace quasi {
+
+int set_error(int code, const std::string& msg) { return fail(code, msg); }
+
+std::string validate_config(const quasi_config& c) {
+  if (!is_axis_len(c.nx) || !is_axis_len(c.ny) || !is_axis_len(c.nz))
+    return "each of nx, ny, nz must be one of 8 16 32 64 96 128 192 256 512";
+  if (c.nz % 16 != 0) return "nz must be a multiple of 16";
+  if ((long)c.nx * c.ny % 16 != 0) return "nx*ny must be a multiple of 16";
+  if (c.variant != QUASI_VARIANT_QUASI && c.variant != QUASI_VARIANT_STB) return "unknown variant";
+  if (c.precision != QUASI_PREC_FP64 && c.precision != QUASI_PREC_FP32) return "unknown precision";
+  if (c.emulate_ranks < 1 || c.nx % c.emulate_ranks != 0) return "emulate_ranks must divide nx";
+  if (c.emulate_ranks > 1 && c.emulate_ranks % 2 != 0)
+    return "emulate_ranks must be 1 or even (the reference's halo exchanges need an even rank count)";
+  if (!(c.dt > 0) || !(c.nu_arg > 0) || !(c.q0 > 0) || c.nw <= 0) return "dt, nu, q0 and nw must be positive";
+  return "";
+}
+
+}  // namespace quasi
+
+struct quasi_handle {
+  quasi::EngineBase* eng;
+  quasi_config cfg;
+};
+
+extern "C" {
+
+int quasi_abi_version(void) { return QUASI_ABI_VERSION; }
+
+const char* quasi_last_error(void) { return g_err.c_str(); }
+
+int quasi_config_default(quasi_config* c, int variant, int nx, int ny, int nz) {
+  if (!c) return fail(QUASI_ERR_INVALID, "null config");
+  *c = quasi_config{};
+  c->nx = nx; c->ny = ny; c->nz = nz;
+  c->variant = variant;
+  c->precision = QUASI_PREC_FP64;
+  c->emulate_ranks = 1;
+  c->device = 0;
+  c->alpha = 1.0; c->q0 = 1.0; c->nw = 8;
+  c->ep_arg = 675.0;   /* epsilon = -0.675: the one-mode coexistence value */
+  c->nu_arg = 1.0;
+  c->divv_switch = 200;            /* quasi.cpp:161 */
+  c->q_pert = 0.5;                 /* quasi-stb.cpp:157 */
+  if (variant == QUASI_VARIANT_QUASI) {
+    c->gamma = 1.0; c->beta = 2.0;                 /* quasi.cpp:183-184 */
+    c->amp = 1.34164; c->rho_0 = 0.005; c->kp = 0.5;  /* quasi.cpp:194-196 */
+    c->rho_m = 0.0;                                 /* derived: rho_s / 2 */
+    c->dt = 0.001;                                  /* quasi.cpp:203 */
+  } else if (variant == QUASI_VARIANT_STB) {
+    c->gamma = 3.0; c->beta = 0.4;                  /* quasi-stb.cpp:177-178 */
+    c->amp = 0.3464101615; c->rho_0 = 0.1; c->kp = 0.5;
+    c->rho_m = 0.5;                                 /* quasi-stb.cpp:197 */
+    c->dt = 0.0005;                                 /* quasi-stb.cpp:203 */
+  } else {
+    return fail(QUASI_ERR_INVALID, "unknown variant");
+  }
+  return QUASI_OK;
+}
+
+int quasi_create(const quasi_config* cfg, quasi_handle** out) {
+  if (!cfg || !out) return fail(QUASI_ERR_INVALID, "null argument");
+  *out = nullptr;
+  std::string why = quasi::validate_config(*cfg);
+  if (!why.empty()) return fail(QUASI_ERR_INVALID, why);
+  int rc = device_check(cfg->device);
+  if (rc) return rc;
+  std::string err;
+  quasi::EngineBase* e = cfg->precision == QUASI_PREC_FP64 ? quasi::make_engine_f64(*cfg, err)
+                                                           : quasi::make_engine_f32(*cfg, err);
+  if (!e) return fail(err.find("allocation") != std::string::npos ? QUASI_ERR_NOMEM : QUASI_ERR_CUDA, err);
+  *out = new (std::nothrow) quasi_handle{e, *cfg};
+  if (!*out) {
+    delete e;
+    return fail(QUASI_ERR_NOMEM, "host allocation failed");
+  }
+  return QUASI_OK;
+}
+
+int quasi_destroy(quasi_handle* h) {
+  if (!h) return QUASI_OK;
+  delete h->eng;
+  delete h;
+  return QUASI_OK;
+}
+
+#define QUASI_CALL(h, expr)                                     \
+  do {                                                          \
+    if (!(h)) return fail(QUASI_ERR_INVALID, "null handle");    \
+    int rc_ = (expr);                                           \
+    if (rc_) return fail(rc_, (h)->eng->err);                   \
+    return QUASI_OK;                                            \
+  } while (0)
+
+int quasi_set_psi(quasi_handle* h, const double* host_psi) {
+  if (!host_psi) return fail(QUASI_ERR_INVALID, "null psi");
+  QUASI_CALL(h, h->eng->set_psi(host_psi));
+}
+
+int quasi_init(quasi_handle* h) { QUASI_CALL(h, h->eng->init()); }
+
+int quasi_step(quasi_handle* h, int nsteps) { QUASI_CALL(h, h->eng->step(nsteps, nullptr)); }
+
+int quasi_step_timed(quasi_handle* h, int nsteps, double* device_ms) {
+  if (!device_ms) return fail(QUASI_ERR_INVALID, "null device_ms");
+  QUASI_CALL(h, h->eng->step(nsteps, device_ms));
+}
+
+int quasi_step_count(const quasi_handle* h, long* nloop) {
+  if (!h || !nloop) return fail(QUASI_ERR_INVALID, "null argument");
+  *nloop = h->eng->nloop();
+  return QUASI_OK;
+}
+
+int quasi_get_field(quasi_handle* h, int field, double* host_out) {
+  if (!host_out) return fail(QUASI_ERR_INVALID, "null output");
+  QUASI_CALL(h, h->eng->get_field(field, host_out));
+}
+
+int quasi_diagnostics(quasi_handle* h, double out[3]) {
+  if (!out) return fail(QUASI_ERR_INVALID, "null output");
+  QUASI_CALL(h, h->eng->diagnostics(out));
+}
+
+int quasi_growth_rate(quasi_handle* h, double* out) {
+  if (!out) return fail(QUASI_ERR_INVALID, "null output");
+  QUASI_CALL(h, h->eng->growth_rate(out));
+}
+
+int quasi_save(quasi_handle* h, const char* path) {
+  if (!path) return fail(QUASI_ERR_INVALID, "null path");
+  QUASI_CALL(h, h->eng->save(path));
+}
+
+int quasi_load(quasi_handle* h, const char* path) {
+  if (!path) return fail(QUASI_ERR_INVALID, "null path");
+  QUASI_CALL(h, h->eng->load(path));
+}
+
+}  // extern "C"

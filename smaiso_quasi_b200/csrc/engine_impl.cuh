@@ -1,0 +1,356 @@
+// Engine<T>: one simulation instance on one GPU.  Included by engine_f64.cu
+// and engine_f32.cu, which instantiate it for double and float.
+#pragma once
+#include <cstdint>
+#include <fstream>
+
+#include "engine.cuh"
+
+namespace quasi {
+
+// ---------------------------------------------------------------------------
+// FP64 reductions: L1 numerator/denominator, mass, energy (quasi.cpp:1983-1996)
+// ---------------------------------------------------------------------------
+constexpr int kDiagBlocks = 592;   // 4 x 148 SMs
+constexpr int kDiagThreads = 256;
+
+template <typename T>
+__global__ void __launch_bounds__(kDiagThreads) diag_partial_kernel(const T* psi, const T* psi_old, const T* rho,
+                                                                    const T* df, double ep, double alpha, double beta,
+                                                                    double gamma, int with_energy, size_t n,
+                                                                    double* partial) {
+  double a = 0, b = 0, m = 0, en = 0;
+  for (size_t id = blockIdx.x * size_t(blockDim.x) + threadIdx.x; id < n; id += size_t(gridDim.x) * blockDim.x) {
+    const double ps = psi[id];
+    a += fabs(ps - double(psi_old[id]));
+    b += fabs(ps);
+    const double r = rho[id];
+    m += r;
+    if (with_energy) {
+      const double d = df[id], p2 = ps * ps;
+      en += r * (-0.5 * ep * p2 + 0.5 * alpha * d * d - 0.25 * beta * p2 * p2 + (gamma / 6) * p2 * p2 * p2);
+    }
+  }
+  __shared__ double red[4][kDiagThreads / 32];
+  double v[4] = {a, b, m, en};
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    for (int off = 16; off > 0; off >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], off);
+    if ((threadIdx.x & 31) == 0) red[q][threadIdx.x >> 5] = v[q];
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    double s = 0;
+    for (int w = 0; w < kDiagThreads / 32; ++w) s += red[threadIdx.x][w];
+    partial[blockIdx.x * 4 + threadIdx.x] = s;
+  }
+}
+
+static __global__ void diag_final_kernel(const double* partial, int nblocks, double* out) {
+  // fixed-order sums: deterministic run to run
+  if (threadIdx.x < 4) {
+    double s = 0;
+    for (int b = 0; b < nblocks; ++b) s += partial[b * 4 + threadIdx.x];
+    out[threadIdx.x] = s;
+  }
+}
+
+template <typename T>
+class Engine : public EngineBase {
+ public:
+  static constexpr int kFields = 32;
+
+  explicit Engine(const quasi_config& cfg) : cfg_(cfg) {}
+
+  ~Engine() override {
+    if (dev_ok_) cudaSetDevice(cfg_.device);
+    if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+    if (slab_) cudaFree(slab_);
+    if (tabs_) cudaFree(tabs_);
+    if (nloop_dev_) cudaFree(nloop_dev_);
+    if (partial_) cudaFree(partial_);
+    if (host_stage_) cudaFreeHost(host_stage_);
+    for (auto& t : tw_) t.release();
+    if (ev0_) cudaEventDestroy(ev0_);
+    if (ev1_) cudaEventDestroy(ev1_);
+    if (stream_) cudaStreamDestroy(stream_);
+  }
+
+  int create() {
+    if (!cuda_ok(cudaSetDevice(cfg_.device), "cudaSetDevice")) return QUASI_ERR_NODEVICE;
+    dev_ok_ = true;
+    g_ = Geom{cfg_.nx, cfg_.ny, cfg_.nz};
+    n_ = size_t(g_.nx) * g_.ny * g_.nz;
+    if (!cuda_ok(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "stream")) return QUASI_ERR_CUDA;
+    if (!cuda_ok(cudaEventCreate(&ev0_), "event") || !cuda_ok(cudaEventCreate(&ev1_), "event")) return QUASI_ERR_CUDA;
+    const size_t bytes = size_t(kFields) * n_ * sizeof(T);
+    if (cudaMalloc(&slab_, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      err = "device allocation of " + std::to_string(bytes) + " bytes failed";
+      return QUASI_ERR_NOMEM;
+    }
+    if (!cuda_ok(cudaMemset(slab_, 0, bytes), "memset")) return QUASI_ERR_CUDA;
+    if (!cuda_ok(cudaMalloc(&nloop_dev_, sizeof(int)), "malloc") || !cuda_ok(cudaMemset(nloop_dev_, 0, sizeof(int)), "memset"))
+      return QUASI_ERR_CUDA;
+    if (!cuda_ok(cudaMalloc(&partial_, (kDiagBlocks * 4 + 4) * sizeof(double)), "malloc")) return QUASI_ERR_CUDA;
+    if (!cuda_ok(cudaMallocHost(&host_stage_, n_ * sizeof(T) + 64), "host alloc")) return QUASI_ERR_NOMEM;
+    // wavenumber tables, quasi.cpp:397-431
+    const int len[3] = {g_.nx, g_.ny, g_.nz};
+    std::vector<double> h;
+    for (int a = 0; a < 3; ++a) {
+      const int n = len[a];
+      const double L = n * 2.0 * M_PI / (cfg_.q0 * cfg_.nw);
+      const double d = L / n;
+      for (int i = 0; i < n; ++i) h.push_back(1.0 * M_PI * i / (d * n));
+      for (int i = 0; i < n; ++i) h.push_back(1.0 * M_PI * (i + 1) / (d * n));
+    }
+    if (!cuda_ok(cudaMalloc(&tabs_, h.size() * sizeof(double)), "malloc")) return QUASI_ERR_CUDA;
+    if (!cuda_ok(cudaMemcpy(tabs_, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice), "memcpy"))
+      return QUASI_ERR_CUDA;
+    for (int a = 0; a < 3; ++a)
+      if (!cuda_ok(tw_[a].upload(len[a]), "twiddles")) return QUASI_ERR_CUDA;
+    for (int a = 0; a < 3; ++a) tb_.t[a] = tw_[a].tables();
+    build_ctx(h);
+    return QUASI_OK;
+  }
+
+  int set_psi(const double* host) override {
+    T* st = static_cast<T*>(host_stage_);
+    for (size_t i = 0; i < n_; ++i) st[i] = T(host[i]);
+    if (!cuda_ok(cudaMemcpyAsync(c_.psi, st, n_ * sizeof(T), cudaMemcpyHostToDevice, stream_), "H2D")) return QUASI_ERR_CUDA;
+    if (!cuda_ok(cudaStreamSynchronize(stream_), "sync")) return QUASI_ERR_CUDA;
+    have_psi_ = true;
+    initialized_ = false;
+    return QUASI_OK;
+  }
+
+  int init() override {
+    if (!have_psi_) { err = "quasi_init before quasi_set_psi"; return QUASI_ERR_STATE; }
+    if (!cuda_ok(enqueue_init<T>(c_, tb_, nloop_dev_, stream_), "init")) return QUASI_ERR_CUDA;
+    if (!cuda_ok(cudaStreamSynchronize(stream_), "init sync")) return QUASI_ERR_CUDA;
+    nloop_ = 0;
+    initialized_ = true;
+    return QUASI_OK;
+  }
+
+  int step(int nsteps, double* device_ms) override {
+    if (!initialized_) { err = "quasi_step before quasi_init"; return QUASI_ERR_STATE; }
+    if (nsteps < 0) { err = "nsteps < 0"; return QUASI_ERR_INVALID; }
+    if (!graph_exec_) {
+      int rc = capture();
+      if (rc) return rc;
+    }
+    if (device_ms && !cuda_ok(cudaEventRecord(ev0_, stream_), "event")) return QUASI_ERR_CUDA;
+    for (int s = 0; s < nsteps; ++s)
+      if (!cuda_ok(cudaGraphLaunch(graph_exec_, stream_), "graph launch")) return QUASI_ERR_CUDA;
+    if (device_ms && !cuda_ok(cudaEventRecord(ev1_, stream_), "event")) return QUASI_ERR_CUDA;
+    if (!cuda_ok(cudaStreamSynchronize(stream_), "step sync")) return QUASI_ERR_CUDA;
+    if (device_ms) {
+      float ms = 0;
+      if (!cuda_ok(cudaEventElapsedTime(&ms, ev0_, ev1_), "elapsed")) return QUASI_ERR_CUDA;
+      *device_ms = ms;
+    }
+    nloop_ += nsteps;
+    return QUASI_OK;
+  }
+
+  int get_field(int field, double* host) override {
+    const T* src = field_ptr(field);
+    if (!src) { err = "unknown or unavailable field " + std::to_string(field); return QUASI_ERR_INVALID; }
+    T* st = static_cast<T*>(host_stage_);
+    if (!cuda_ok(cudaMemcpyAsync(st, src, n_ * sizeof(T), cudaMemcpyDeviceToHost, stream_), "D2H")) return QUASI_ERR_CUDA;
+    if (!cuda_ok(cudaStreamSynchronize(stream_), "sync")) return QUASI_ERR_CUDA;
+    for (size_t i = 0; i < n_; ++i) host[i] = double(st[i]);
+    return QUASI_OK;
+  }
+
+  int diagnostics(double out[3]) override {
+    if (!initialized_) { err = "diagnostics before quasi_init"; return QUASI_ERR_STATE; }
+    const int energy = cfg_.variant == QUASI_VARIANT_QUASI;
+    diag_partial_kernel<T><<<kDiagBlocks, kDiagThreads, 0, stream_>>>(c_.psi, c_.psi_old, c_.rho, c_.df, c_.ep, c_.alpha,
+                                                                      c_.beta, c_.gamma, energy, n_, partial_);
+    diag_final_kernel<<<1, 32, 0, stream_>>>(partial_, kDiagBlocks, partial_ + kDiagBlocks * 4);
+    double r[4];
+    if (!cuda_ok(cudaMemcpyAsync(r, partial_ + kDiagBlocks * 4, sizeof(r), cudaMemcpyDeviceToHost, stream_), "D2H"))
+      return QUASI_ERR_CUDA;
+    if (!cuda_ok(cudaStreamSynchronize(stream_), "sync")) return QUASI_ERR_CUDA;
+    const double dx = (g_.nx * 2.0 * M_PI / (cfg_.q0 * cfg_.nw)) / g_.nx;
+    out[0] = r[0] / (c_.dt * r[1]);
+    out[1] = r[2] * dx * dx * dx;
+    out[2] = energy ? r[3] * dx * dx * dx : 0.0;
+    return QUASI_OK;
+  }
+
+  int growth_rate(double* out) override {
+    const double vq1 = M_PI * 1 / ((g_.nz * 2.0 * M_PI / (cfg_.q0 * cfg_.nw)) / g_.nz * g_.nz);
+    const int i = (int)std::lround(cfg_.q_pert / vq1), k = (int)std::lround(cfg_.q0 / vq1);
+    if (i < 0 || i >= g_.nx || k < 0 || k >= g_.nz) { err = "growth probe mode outside the grid"; return QUASI_ERR_INVALID; }
+    const size_t id = (size_t(i) * g_.ny + 0) * g_.nz + k;
+    T a, b;
+    if (!cuda_ok(cudaMemcpyAsync(&a, c_.psiq + id, sizeof(T), cudaMemcpyDeviceToHost, stream_), "D2H") ||
+        !cuda_ok(cudaMemcpyAsync(&b, c_.psiq_old + id, sizeof(T), cudaMemcpyDeviceToHost, stream_), "D2H") ||
+        !cuda_ok(cudaStreamSynchronize(stream_), "sync"))
+      return QUASI_ERR_CUDA;
+    *out = (double(a) - double(b)) / (cfg_.dt * double(b));
+    return QUASI_OK;
+  }
+
+  // Binary checkpoint: header + the carried state in T.
+  int save(const char* path) override {
+    if (!initialized_) { err = "save before quasi_init"; return QUASI_ERR_STATE; }
+    std::ofstream f(path, std::ios::binary);
+    if (!f) { err = std::string("cannot open ") + path; return QUASI_ERR_IO; }
+    Header hd = header();
+    f.write(reinterpret_cast<const char*>(&hd), sizeof(hd));
+    for (T* p : carried()) {
+      if (!cuda_ok(cudaMemcpy(host_stage_, p, n_ * sizeof(T), cudaMemcpyDeviceToHost), "D2H")) return QUASI_ERR_CUDA;
+      f.write(static_cast<const char*>(host_stage_), n_ * sizeof(T));
+    }
+    if (!f) { err = std::string("write failed: ") + path; return QUASI_ERR_IO; }
+    return QUASI_OK;
+  }
+
+  int load(const char* path) override {
+    std::ifstream f(path, std::ios::binary);
+    if (!f) { err = std::string("cannot open ") + path; return QUASI_ERR_IO; }
+    Header hd{}, want = header();
+    f.read(reinterpret_cast<char*>(&hd), sizeof(hd));
+    if (!f || std::memcmp(hd.magic, want.magic, 8) != 0) { err = "not a quasi checkpoint"; return QUASI_ERR_IO; }
+    if (hd.nx != want.nx || hd.ny != want.ny || hd.nz != want.nz || hd.variant != want.variant ||
+        hd.elem != want.elem) {
+      err = "checkpoint grid/variant/precision does not match the handle";
+      return QUASI_ERR_IO;
+    }
+    for (T* p : carried()) {
+      f.read(static_cast<char*>(host_stage_), n_ * sizeof(T));
+      if (!f) { err = "checkpoint is truncated"; return QUASI_ERR_IO; }
+      if (!cuda_ok(cudaMemcpy(p, host_stage_, n_ * sizeof(T), cudaMemcpyHostToDevice), "H2D")) return QUASI_ERR_CUDA;
+    }
+    int nl = int(hd.nloop);
+    if (!cuda_ok(cudaMemcpy(nloop_dev_, &nl, sizeof(int), cudaMemcpyHostToDevice), "H2D")) return QUASI_ERR_CUDA;
+    nloop_ = hd.nloop;
+    have_psi_ = initialized_ = true;
+    return QUASI_OK;
+  }
+
+  long nloop() const override { return nloop_; }
+
+ private:
+  struct Header {
+    char magic[8];
+    int32_t nx, ny, nz, variant, elem, pad;
+    int64_t nloop;
+  };
+  Header header() const {
+    Header h{};
+    std::memcpy(h.magic, "QUASICK1", 8);
+    h.nx = g_.nx; h.ny = g_.ny; h.nz = g_.nz; h.variant = cfg_.variant; h.elem = int(sizeof(T));
+    h.nloop = nloop_;
+    return h;
+  }
+  std::vector<T*> carried() {
+    return {c_.psiq, c_.psiq_old, c_.Nq, c_.Nq_old, c_.rhoq, c_.rho_old, c_.rho, c_.vx, c_.vy, c_.vz,
+            c_.divv, c_.divvq, c_.psi, c_.psi_old, c_.p, c_.df};
+  }
+
+  bool cuda_ok(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return true;
+    err = std::string(what) + ": " + cudaGetErrorString(e);
+    return false;
+  }
+
+  void build_ctx(const std::vector<double>&) {
+    T* f = static_cast<T*>(slab_);
+    auto next = [&]() { T* p = f; f += n_; return p; };
+    c_.g = g_;
+    const double* t = tabs_;
+    c_.vqx = t;                 c_.vsx = t + g_.nx;
+    c_.vqy = t + 2 * g_.nx;     c_.vsy = c_.vqy + g_.ny;
+    c_.vqz = t + 2 * g_.nx + 2 * g_.ny; c_.vsz = c_.vqz + g_.nz;
+    const bool quasi = cfg_.variant == QUASI_VARIANT_QUASI;
+    c_.ep = -0.001 * cfg_.ep_arg;                                   // quasi.cpp:187
+    c_.alpha = cfg_.alpha; c_.beta = cfg_.beta; c_.gamma = cfg_.gamma; c_.q0 = cfg_.q0;
+    c_.kp = cfg_.kp; c_.rho0 = cfg_.rho_0;
+    c_.rho_s = cfg_.kp * cfg_.amp + cfg_.rho_0;                     // quasi.cpp:197
+    c_.rho_m = cfg_.rho_m > 0 ? cfg_.rho_m : c_.rho_s / 2;          // quasi.cpp:198
+    c_.nu = quasi ? cfg_.nu_arg : 0.1 * cfg_.nu_arg;                // quasi.cpp:192, quasi-stb.cpp:191
+    c_.dt = cfg_.dt;
+    c_.scale = 0.125 / (double(g_.nx) * g_.ny * g_.nz);              // quasi.cpp:219
+    c_.variant = cfg_.variant;
+    c_.divv_switch = cfg_.divv_switch;
+    c_.n0 = g_.nx / (cfg_.emulate_ranks > 0 ? cfg_.emulate_ranks : 1);
+    c_.nloop = nloop_dev_;
+    c_.store_dtpsi = quasi ? 0 : 1;
+    c_.psiq = next(); c_.psiq_old = next(); c_.Nq = next(); c_.Nq_old = next(); c_.rhoq = next();
+    c_.divvq = next(); c_.Sx = next(); c_.Sy = next(); c_.Sz = next();
+    c_.psi = next(); c_.psi_old = next(); c_.rho = next(); c_.rho_old = next();
+    c_.vx = next(); c_.vy = next(); c_.vz = next(); c_.divv = next(); c_.p = next();
+    c_.df = next(); c_.lap = next(); c_.gx = next(); c_.gy = next(); c_.gz = next();
+    c_.rdx = next(); c_.rdy = next(); c_.rdz = next(); c_.ldx = next(); c_.ldy = next(); c_.ldz = next();
+    c_.sh = next(); c_.dtpsi = next(); c_.tmp = next();
+  }
+
+  const T* field_ptr(int f) const {
+    switch (f) {
+      case QUASI_FIELD_PSI: return c_.psi;
+      case QUASI_FIELD_RHO: return c_.rho;
+      case QUASI_FIELD_VX: return c_.vx;
+      case QUASI_FIELD_VY: return c_.vy;
+      case QUASI_FIELD_VZ: return c_.vz;
+      case QUASI_FIELD_P: return c_.p;
+      case QUASI_FIELD_DIVV: return c_.divv;
+      case QUASI_FIELD_PSIQ: return c_.psiq;
+      case QUASI_FIELD_PSIQ_OLD: return c_.psiq_old;
+      case QUASI_FIELD_DTPSI: return cfg_.variant == QUASI_VARIANT_STB ? c_.dtpsi : nullptr;
+      case QUASI_FIELD_DF: return c_.df;
+      default: return nullptr;
+    }
+  }
+
+  int capture() {
+    cudaGraph_t graph = nullptr;
+    if (!cuda_ok(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture"))
+      return QUASI_ERR_CUDA;
+    cudaError_t e = enqueue_step<T>(c_, tb_, nloop_dev_, stream_);
+    cudaError_t e2 = cudaStreamEndCapture(stream_, &graph);
+    if (!cuda_ok(e, "enqueue step") || !cuda_ok(e2, "end capture")) {
+      if (graph) cudaGraphDestroy(graph);
+      return QUASI_ERR_CUDA;
+    }
+    e = cudaGraphInstantiate(&graph_exec_, graph, 0);
+    cudaGraphDestroy(graph);
+    if (!cuda_ok(e, "graph instantiate")) { graph_exec_ = nullptr; return QUASI_ERR_CUDA; }
+    return QUASI_OK;
+  }
+
+  quasi_config cfg_;
+  Geom g_{};
+  size_t n_ = 0;
+  bool dev_ok_ = false, have_psi_ = false, initialized_ = false;
+  cudaStream_t stream_ = nullptr;
+  cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+  void* slab_ = nullptr;
+  double* tabs_ = nullptr;
+  int* nloop_dev_ = nullptr;
+  double* partial_ = nullptr;
+  void* host_stage_ = nullptr;
+  DevTwiddles<T> tw_[3];
+  AxisTables<T> tb_{};
+  StepCtx<T> c_{};
+  cudaGraphExec_t graph_exec_ = nullptr;
+  long nloop_ = 0;
+};
+
+template <typename T>
+EngineBase* make_engine(const quasi_config& cfg, std::string& err) {
+  auto* e = new Engine<T>(cfg);
+  int rc = e->create();
+  if (rc) {
+    err = e->err;
+    delete e;
+    return nullptr;
+  }
+  return e;
+}
+
+}  // namespace quasi

@@ -1,0 +1,166 @@
+"""The CUDA step (through the C ABI) against the oracle and the reference's
+own dumps (tests/golden)."""
+import json
+import pathlib
+
+import numpy as np
+import pytest
+
+from oracle import quasi_oracle as qo
+
+pytestmark = pytest.mark.gpu
+GOLDEN = pathlib.Path(__file__).resolve().parent / "golden"
+
+# FP64: same arithmetic as the reference up to FMA contraction and transform
+# round-off; the bar is 1e-12 relative L2 (v: of the velocity vector).
+TOL64 = 1e-12
+
+
+def rel(a, b):
+    nb = np.linalg.norm(b)
+    return np.linalg.norm(a - b) / nb if nb else np.linalg.norm(a)
+
+
+def vec_err(got, ref):
+    num = sum(np.linalg.norm(got[c] - ref[c]) ** 2 for c in ("vx", "vy", "vz"))
+    den = sum(np.linalg.norm(ref[c]) ** 2 for c in ("vx", "vy", "vz"))
+    return np.sqrt(num / den) if den else np.sqrt(num)
+
+
+def make_pair(variant, grid, ranks=1, precision="fp64", ic="planar", seed=7):
+    import smaiso_quasi_b200 as q
+    cfg = q.default_config(variant, *grid, emulate_ranks=ranks, precision=precision)
+    m = qo.Model(nx=grid[0], ny=grid[1], nz=grid[2], emulate_ranks=ranks) if variant == "quasi" else \
+        qo.Model.stb(nx=grid[0], ny=grid[1], nz=grid[2], emulate_ranks=ranks)
+    psi0 = qo.ic_field(m, ic, seed=seed)
+    sim = q.Simulation(cfg)
+    sim.set_psi(psi0)
+    sim.init()
+    o = qo.QuasiOracle(m)
+    o.set_psi(psi0)
+    o.init()
+    return sim, o
+
+
+def compare(sim, o, tol):
+    got = {f: sim.field(f) for f in ("psi", "rho", "vx", "vy", "vz", "p", "divv", "psiq")}
+    ref = {"psi": o.psi, "rho": o.rho, "vx": o.velx, "vy": o.vely, "vz": o.velz, "p": o.p, "divv": o.divv,
+           "psiq": o.psiq}
+    errs = {f: rel(got[f], ref[f]) for f in ("psi", "rho", "p", "psiq")}
+    errs["v"] = vec_err(got, ref)
+    if np.linalg.norm(ref["divv"]) > 0:
+        errs["divv"] = rel(got["divv"], ref["divv"])
+    bad = {k: v for k, v in errs.items() if not v < tol}
+    assert not bad, (errs, tol)
+    return errs
+
+
+def test_init_projection_matches_oracle():
+    sim, o = make_pair("quasi", (16, 16, 32))
+    assert rel(sim.field("psi"), o.psi) < 1e-14
+    assert rel(sim.field("psiq"), o.psiq) < 1e-14
+
+
+@pytest.mark.parametrize("ranks", [1, 2, 4])
+@pytest.mark.parametrize("steps", [1, 2, 10])
+def test_step_fp64_matches_oracle(ranks, steps):
+    sim, o = make_pair("quasi", (16, 16, 32), ranks=ranks)
+    for _ in range(steps):
+        o.step()
+    sim.step(steps)
+    assert sim.nloop == steps
+    compare(sim, o, TOL64)
+    d_gpu, d_ref = np.array(sim.diagnostics()), np.array(o.diagnostics())
+    np.testing.assert_allclose(d_gpu, d_ref, rtol=1e-11)
+
+
+def test_step_fp64_crosses_divv_and_pressure_switches():
+    """Steps 199-203: divv turns on after step 200, the p coupling after 201."""
+    sim, o = make_pair("quasi", (16, 16, 32), ranks=2, seed=11)
+    for _ in range(198):
+        o.step()
+    sim.step(198)
+    for _ in range(5):
+        o.step()
+        sim.step(1)
+        compare(sim, o, 1e-11)
+
+
+@pytest.mark.parametrize("grid", [(32, 32, 64), (24 * 4, 24 * 4, 24 * 8)])
+def test_step_fp64_larger_grids(grid):
+    if grid[0] == 96:
+        grid = (96, 96, 192)
+    sim, o = make_pair("quasi", grid, ranks=2)
+    for _ in range(3):
+        o.step()
+    sim.step(3)
+    compare(sim, o, TOL64)
+
+
+def test_step_stb_matches_oracle():
+    sim, o = make_pair("stb", (16, 16, 32), ranks=2, ic="stb", seed=3)
+    for s in range(6):
+        o.step()
+        sim.step(1)
+        assert rel(sim.field("psi"), o.psi) < TOL64
+        assert rel(sim.field("dtpsi"), o.dtpsi) < 1e-10
+        if s > 0:
+            assert abs(sim.growth_rate() - o.growth_rate()) <= 1e-9 * abs(o.growth_rate())
+
+
+@pytest.mark.parametrize("name", sorted(p.stem for p in GOLDEN.glob("quasi_*.npz")))
+def test_step_matches_reference_dumps(name):
+    """GPU against the reference's own 17-digit dumps (no oracle in between)."""
+    import smaiso_quasi_b200 as q
+    z = np.load(GOLDEN / f"{name}.npz")
+    meta = json.loads(str(z["meta"]))
+    grid = (meta["nx"], meta["ny"], meta["nz"])
+    cfg = q.default_config("quasi", *grid, emulate_ranks=meta["ranks"])
+    psi0 = z["ic"] if "ic" in z.files else q.initial_condition(cfg, "focal_conic", fc_size=float(meta["fc_size"]))
+    sim = q.Simulation(cfg)
+    sim.set_psi(psi0)
+    sim.init()
+    sim.step(meta["steps"])
+    assert rel(sim.field("psi"), z["psi"]) < 1e-12
+    nsl = grid[0] * grid[2]
+    got = {f: sim.field(f)[:, grid[1] // 2, :].reshape(-1) for f in ("vx", "vy", "vz", "rho", "p")}
+    ref = {f: z[f][-1] for f in ("vx", "vy", "vz", "rho", "p")}
+    assert rel(got["rho"], ref["rho"]) < 1e-12
+    assert rel(got["p"], ref["p"]) < 1e-10
+    assert vec_err(got, ref) < 1e-11
+    assert len(got["vx"]) == nsl
+
+
+def test_fp32_error_vs_fp64():
+    """The FP32 form against the FP64 form on the same GPU after 50 steps."""
+    import smaiso_quasi_b200 as q
+    grid = (32, 32, 64)
+    cfg64 = q.default_config("quasi", *grid)
+    cfg32 = q.default_config("quasi", *grid, precision="fp32")
+    psi0 = q.initial_condition(cfg64, "planar", seed=5)
+    sims = []
+    for cfg in (cfg64, cfg32):
+        s = q.Simulation(cfg)
+        s.set_psi(psi0)
+        s.init()
+        s.step(50)
+        sims.append(s)
+    e_psi = rel(sims[1].field("psi"), sims[0].field("psi"))
+    assert e_psi < 1e-5, e_psi
+
+
+def test_checkpoint_round_trip(tmp_path):
+    import smaiso_quasi_b200 as q
+    cfg = q.default_config("quasi", 16, 16, 32)
+    psi0 = q.initial_condition(cfg, "planar", seed=2)
+    a = q.Simulation(cfg)
+    a.set_psi(psi0)
+    a.init()
+    a.step(5)
+    a.save(tmp_path / "ck.bin")
+    a.step(7)
+    b = q.Simulation(cfg)
+    b.load(tmp_path / "ck.bin")
+    assert b.nloop == 5
+    b.step(7)
+    assert np.array_equal(a.field("psi"), b.field("psi"))
