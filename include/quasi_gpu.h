@@ -117,6 +117,15 @@ QUASI_API int quasi_step(quasi_handle* h, int nsteps);
  * *device_ms receives the elapsed device time of the nsteps steps. */
 QUASI_API int quasi_step_timed(quasi_handle* h, int nsteps, double* device_ms);
 
+/* Kernel launches in one step (kernel nodes of the step's CUDA graph; the
+ * graph is captured by the first quasi_step).  No reference counterpart. */
+QUASI_API int quasi_step_kernels(quasi_handle* h, int* launches);
+
+/* Average device time of one plain in-place axis pass (axis 0 = x, 1 = y,
+ * 2 = z) over `reps` back-to-back launches on the handle's stream, timed
+ * with CUDA events; operates on a scratch field.  For roofline reporting. */
+QUASI_API int quasi_time_axis_pass(quasi_handle* h, int axis, int reps, double* avg_ms);
+
 /* Steps taken since quasi_init (the reference's nLoop). */
 QUASI_API int quasi_step_count(const quasi_handle* h, long* nloop);
 

@@ -149,6 +149,16 @@ int quasi_step_count(const quasi_handle* h, long* nloop) {
   return QUASI_OK;
 }
 
+int quasi_step_kernels(quasi_handle* h, int* launches) {
+  if (!launches) return fail(QUASI_ERR_INVALID, "null output");
+  QUASI_CALL(h, h->eng->step_kernels(launches));
+}
+
+int quasi_time_axis_pass(quasi_handle* h, int axis, int reps, double* avg_ms) {
+  if (!avg_ms) return fail(QUASI_ERR_INVALID, "null output");
+  QUASI_CALL(h, h->eng->time_axis_pass(axis, reps, avg_ms));
+}
+
 int quasi_get_field(quasi_handle* h, int field, double* host_out) {
   if (!host_out) return fail(QUASI_ERR_INVALID, "null output");
   QUASI_CALL(h, h->eng->get_field(field, host_out));

@@ -26,6 +26,8 @@ class EngineBase {
   virtual int save(const char* path) = 0;
   virtual int load(const char* path) = 0;
   virtual long nloop() const = 0;
+  virtual int step_kernels(int* n) = 0;
+  virtual int time_axis_pass(int axis, int reps, double* avg_ms) = 0;
   std::string err;
 };
 

@@ -235,6 +235,36 @@ class Engine : public EngineBase {
 
   long nloop() const override { return nloop_; }
 
+  int step_kernels(int* n) override {
+    if (!graph_exec_) {
+      if (!initialized_) { err = "step graph not captured yet (call quasi_init)"; return QUASI_ERR_STATE; }
+      int rc = capture();
+      if (rc) return rc;
+    }
+    *n = graph_kernels_;
+    return QUASI_OK;
+  }
+
+  int time_axis_pass(int axis, int reps, double* avg_ms) override {
+    if (axis < 0 || axis > 2 || reps < 1) { err = "axis must be 0..2 and reps >= 1"; return QUASI_ERR_INVALID; }
+    T* d = c_.tmp;
+    auto one = [&]() -> cudaError_t {
+      if (axis == 0) return launch_pass<T, 0>(g_, E01, tb_.t[0], LoadField<T>{g_, d}, StoreField<T>{g_, d}, stream_);
+      if (axis == 1) return launch_pass<T, 1>(g_, E01, tb_.t[1], LoadField<T>{g_, d}, StoreField<T>{g_, d}, stream_);
+      return launch_pass<T, 2>(g_, E01, tb_.t[2], LoadField<T>{g_, d}, StoreField<T>{g_, d}, stream_);
+    };
+    if (!cuda_ok(one(), "pass")) return QUASI_ERR_CUDA;   // warm
+    if (!cuda_ok(cudaEventRecord(ev0_, stream_), "event")) return QUASI_ERR_CUDA;
+    for (int r = 0; r < reps; ++r)
+      if (!cuda_ok(one(), "pass")) return QUASI_ERR_CUDA;
+    if (!cuda_ok(cudaEventRecord(ev1_, stream_), "event") || !cuda_ok(cudaEventSynchronize(ev1_), "sync"))
+      return QUASI_ERR_CUDA;
+    float ms = 0;
+    if (!cuda_ok(cudaEventElapsedTime(&ms, ev0_, ev1_), "elapsed")) return QUASI_ERR_CUDA;
+    *avg_ms = double(ms) / reps;
+    return QUASI_OK;
+  }
+
  private:
   struct Header {
     char magic[8];
@@ -317,6 +347,15 @@ class Engine : public EngineBase {
       if (graph) cudaGraphDestroy(graph);
       return QUASI_ERR_CUDA;
     }
+    size_t nodes = 0;
+    cudaGraphGetNodes(graph, nullptr, &nodes);
+    std::vector<cudaGraphNode_t> list(nodes);
+    cudaGraphGetNodes(graph, list.data(), &nodes);
+    graph_kernels_ = 0;
+    for (auto nd : list) {
+      cudaGraphNodeType t;
+      if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++graph_kernels_;
+    }
     e = cudaGraphInstantiate(&graph_exec_, graph, 0);
     cudaGraphDestroy(graph);
     if (!cuda_ok(e, "graph instantiate")) { graph_exec_ = nullptr; return QUASI_ERR_CUDA; }
@@ -338,6 +377,7 @@ class Engine : public EngineBase {
   AxisTables<T> tb_{};
   StepCtx<T> c_{};
   cudaGraphExec_t graph_exec_ = nullptr;
+  int graph_kernels_ = 0;
   long nloop_ = 0;
 };
 

@@ -163,150 +163,207 @@ struct Tables {
   const Cx<T>* quarter;
 };
 
-// One Stockham stage: src -> dst, n = current sub-length, s = stride, radix R.
-// Work items: G complex pencils x (N / R) butterflies, pencil index fastest so
-// that neighbouring threads touch the same offset of neighbouring pencils
-// (pencil stride ld = N + 1 keeps those in distinct shared-memory banks).
-template <typename T, int N, int R>
-QHD void stockham_stage(int w, int G, const Cx<T>* src, Cx<T>* dst, int n, int s, int ld, Tables<T> tb) {
-  const int g = w % G, b = w / G;
-  const int m = n / R;
-  const int p = b / s, q = b - p * s;
-  const Cx<T>* sp = src + g * ld;
-  Cx<T>* dp = dst + g * ld;
-  Cx<T> a[R];
-#pragma unroll
-  for (int t = 0; t < R; ++t) a[t] = sp[q + s * (p + t * m)];
-  Dft<T, R>::run(a);
-  const int step = (N / n) * p;   // W_n^{p u} = root[(N/n) p u]
-#pragma unroll
-  for (int u = 0; u < R; ++u) {
-    Cx<T> v = a[u];
-    if (u && p) v = cmul(v, tb.root[step * u]);   // step*u <= (m-1)(R-1)N/n < N
-    dp[q + s * (R * p + u)] = v;
-  }
-}
-
 // ---------------------------------------------------------------------------
-// The tile: P real pencils of length N at rt[p * ldr + n] (real layout) and
-// G = P/2 complex pencils at cb[g * ldc + n].  Both buffers are the same
-// byte size and alternate roles.
-// ---------------------------------------------------------------------------
-
-// (1) forward kinds: real tile -> packed complex (Makhoul reorder, DST sign)
-template <typename T, int N>
-QHD void fwd_pack(int w, int G, int kind, const T* rt, int ldr, Cx<T>* cb, int ldc) {
-  // w in [0, G * N/2)
-  const int g = w % G, t = w / G;
-  const T* a = rt + (2 * g) * ldr;
-  const T* b = rt + (2 * g + 1) * ldr;
-  T a0 = a[2 * t], a1 = a[2 * t + 1], b0 = b[2 * t], b1 = b[2 * t + 1];
-  if (kind == O10) { a1 = -a1; b1 = -b1; }
-  cb[g * ldc + t] = Cx<T>{a0, b0};
-  cb[g * ldc + N - 1 - t] = Cx<T>{a1, b1};
-}
-
-// (2) forward kinds: complex spectrum -> two real pencils
-template <typename T, int N>
-QHD void fwd_unpack(int w, int G, int kind, const Cx<T>* cb, int ldc, T* rt, int ldr, Tables<T> tb) {
-  // w in [0, G * N)
-  const int g = w % G, k = w / G;
-  const Cx<T> zk = cb[g * ldc + k];
-  const Cx<T> zr = conj(cb[g * ldc + (k == 0 ? 0 : N - k)]);
-  // V_a = (zk + zr)/2, V_b = (zk - zr)/(2i); y = 2 Re(quarter[k] V)
-  const Cx<T> va = zk + zr;                    // 2 V_a
-  const Cx<T> d = zk - zr;
-  const Cx<T> vb = {d.y, -d.x};                // 2 V_b
-  const Cx<T> qk = tb.quarter[k];
-  const T ya = qk.x * va.x - qk.y * va.y;      // Re(q * 2V_a) = 2 Re(q V_a)
-  const T yb = qk.x * vb.x - qk.y * vb.y;
-  const int dst = (kind == O10) ? N - 1 - k : k;
-  rt[(2 * g) * ldr + dst] = ya;
-  rt[(2 * g + 1) * ldr + dst] = yb;
-}
-
-// (3) inverse kinds: two real coefficient pencils -> packed complex, conjugated
-//     (the inverse DFT is run as conj(FFT(conj(.))))
-template <typename T, int N>
-QHD void inv_pack(int w, int G, int kind, const T* rt, int ldr, Cx<T>* cb, int ldc, Tables<T> tb) {
-  // w in [0, G * N)
-  const int g = w % G, k = w / G;
-  const T* a = rt + (2 * g) * ldr;
-  const T* b = rt + (2 * g + 1) * ldr;
-  const bool rev = kind == O01;
-  auto at = [&](const T* s, int i) -> T {   // y_i with y_N = 0, reversed for O01
-    return i >= N ? T(0) : s[rev ? N - 1 - i : i];
-  };
-  const T ak = at(a, k), bk = at(b, k);
-  const T an = k ? at(a, N - k) : T(0), bn = k ? at(b, N - k) : T(0);
-  // V = e^{+i pi k/2N} (y_k - i y_{N-k});  packed = V_a + i V_b
-  const Cx<T> e = conj(tb.quarter[k]);
-  const Cx<T> va = cmul(e, Cx<T>{ak, -an});
-  const Cx<T> vb = cmul(e, Cx<T>{bk, -bn});
-  const Cx<T> z = {va.x - vb.y, va.y + vb.x};
-  cb[g * ldc + k] = conj(z);
-}
-
-// (4) inverse kinds: conj(FFT) result -> two real pencils (Makhoul un-reorder)
-template <typename T, int N>
-QHD void inv_unpack(int w, int G, int kind, const Cx<T>* cb, int ldc, T* rt, int ldr) {
-  // w in [0, G * N/2)
-  const int g = w % G, t = w / G;
-  const Cx<T> u0 = conj(cb[g * ldc + t]);
-  const Cx<T> u1 = conj(cb[g * ldc + N - 1 - t]);
-  const T sgn = (kind == O01) ? T(-1) : T(1);
-  rt[(2 * g) * ldr + 2 * t] = u0.x;
-  rt[(2 * g) * ldr + 2 * t + 1] = sgn * u1.x;
-  rt[(2 * g + 1) * ldr + 2 * t] = u0.y;
-  rt[(2 * g + 1) * ldr + 2 * t + 1] = sgn * u1.y;
-}
-
-// ---------------------------------------------------------------------------
-// Whole tile: P = 2G real pencils of length N in buffer `a` (pencil stride
-// LD = tile_ld(N) reals) are transformed with `kind`; `b` is a second buffer
-// of the same size (G pencils of LD complex).  Returns the buffer that holds
-// the result (a or b), real layout, stride LD.
-// `ex.loop(count, f)` runs f(w) for w < count across the CTA and then
-// synchronises (device), or serially (host unit test).
+// In-place tile transform.
+//
+// Tile: P = 2G real pencils of length N at buf[r * LD + n] (reals), LD = N + 1.
+// Complex pencil g (LD complex elements) occupies exactly the bytes of real
+// pencils 2g and 2g+1, so the whole transform runs in ONE buffer: every stage
+// reads all its inputs into registers, the CTA synchronises, then writes.
+// Work items are mapped pencil-fastest (g = w % G) so that neighbouring
+// threads touch the same offset of neighbouring pencils; the odd stride LD
+// keeps those in distinct shared-memory banks.
+//
+// The Makhoul reordering is folded into the first stage's reads (forward
+// kinds, and the inverse kinds' V_k = e^{i pi k/2N}(y_k - i y_{N-k})) and the
+// inverse un-reordering into the last stage's writes; the forward kinds'
+// pairing of Z_k with Z_{N-k} is one extra read/write phase.
 // ---------------------------------------------------------------------------
 QHD constexpr int tile_ld(int n) { return n + 1; }
 
-template <typename T, int N, class Exec>
-QHD T* r2r_tile(Exec& ex, int kind, int G, T* a, T* b, Tables<T> tb) {
-  constexpr RadixPlan plan = radix_plan(N);
-  constexpr int LD = tile_ld(N);
+template <typename T, int N, int G, int NT>
+struct TileFFT {
+  static constexpr RadixPlan plan = radix_plan(N);
+  static constexpr int LD = tile_ld(N);
   static_assert(plan.n_stages > 0, "unsupported transform length");
-  Cx<T>* ca = reinterpret_cast<Cx<T>*>(a);
-  Cx<T>* cbuf = reinterpret_cast<Cx<T>*>(b);
-  if (is_forward(kind)) {
-    ex.loop(G * (N / 2), [&](int w) { fwd_pack<T, N>(w, G, kind, a, LD, cbuf, LD); });
-  } else {
-    ex.loop(G * N, [&](int w) { inv_pack<T, N>(w, G, kind, a, LD, cbuf, LD, tb); });
+
+  // butterflies a thread owns in a radix-R stage
+  template <int R> static constexpr int per_thread() { return (G * (N / R) + NT - 1) / NT; }
+  static constexpr int kMaxRegs = 16;   // complex values a thread holds in any phase
+
+  // ---- stage input element e of complex pencil g --------------------------
+  // first stage: the packed complex sequence is formed from the real tile
+  QHD static Cx<T> first_input(const T* buf, int kind, int g, int e, Tables<T> tb) {
+    const T* a = buf + (2 * g) * LD;
+    const T* b = a + LD;
+    if (is_forward(kind)) {
+      // v_e = x_{2e} (e < N/2), x_{2(N-1-e)+1} (e >= N/2); DST-II negates odd x
+      int src;
+      T sgn = T(1);
+      if (e < N / 2) src = 2 * e;
+      else { src = 2 * (N - 1 - e) + 1; if (kind == O10) sgn = T(-1); }
+      return Cx<T>{sgn * a[src], sgn * b[src]};
+    }
+    // inverse: conj( e^{+i pi k/2N} [(ya_k - i ya_{N-k}) + i (yb_k - i yb_{N-k})] ), y_N = 0,
+    // input reversed for DST-III
+    const int k = e;
+    const bool rev = kind == O01;
+    const int ik = rev ? N - 1 - k : k;
+    const T ak = a[ik], bk = b[ik];
+    T an = T(0), bn = T(0);
+    if (k) {
+      const int in_ = rev ? k - 1 : N - k;   // index of y_{N-k} (reversed: N-1-(N-k))
+      an = a[in_];
+      bn = b[in_];
+    }
+    const Cx<T> q = tb.quarter[k];
+    const Cx<T> ec = {q.x, -q.y};
+    const Cx<T> va = cmul(ec, Cx<T>{ak, -an});
+    const Cx<T> vb = cmul(ec, Cx<T>{bk, -bn});
+    return Cx<T>{va.x - vb.y, -(va.y + vb.x)};
   }
-  Cx<T>* src = cbuf;
-  Cx<T>* dst = ca;
-  int n = N, s = 1;
+
+  // last stage of an inverse kind: FFT output F_k -> u_k = conj(F_k) -> the
+  // two real pencils at the un-reordered positions (DST-III negates odd x)
+  QHD static void last_output_inverse(T* buf, int kind, int g, int k, Cx<T> f) {
+    T* a = buf + (2 * g) * LD;
+    T* b = a + LD;
+    int dst;
+    T sgn = T(1);
+    if (k < N / 2) dst = 2 * k;
+    else { dst = 2 * (N - 1 - k) + 1; if (kind == O01) sgn = T(-1); }
+    a[dst] = sgn * f.x;
+    b[dst] = -sgn * f.y;
+  }
+
+  // ---- one Stockham stage, split into its read and write halves -----------
+  template <int R>
+  struct StageRegs {
+    Cx<T> v[per_thread<R>()][R];
+  };
+
+  template <int R>
+  QHD static void stage_read(int tid, const T* buf, int kind, int n, int s, bool first, Tables<T> tb,
+                             StageRegs<R>& r) {
+    const Cx<T>* cb = reinterpret_cast<const Cx<T>*>(buf);
+    const int m = n / R;
 #pragma unroll
-  for (int st = 0; st < plan.n_stages; ++st) {
-    const int r = plan.r[st];
-    const int cnt = G * (N / r);
-    if (r == 16) ex.loop(cnt, [&](int w) { stockham_stage<T, N, 16>(w, G, src, dst, n, s, LD, tb); });
-    else if (r == 8) ex.loop(cnt, [&](int w) { stockham_stage<T, N, 8>(w, G, src, dst, n, s, LD, tb); });
-    else if (r == 4) ex.loop(cnt, [&](int w) { stockham_stage<T, N, 4>(w, G, src, dst, n, s, LD, tb); });
-    else if (r == 3) ex.loop(cnt, [&](int w) { stockham_stage<T, N, 3>(w, G, src, dst, n, s, LD, tb); });
-    else ex.loop(cnt, [&](int w) { stockham_stage<T, N, 2>(w, G, src, dst, n, s, LD, tb); });
-    n /= r;
-    s *= r;
-    Cx<T>* t = src; src = dst; dst = t;
+    for (int c = 0; c < per_thread<R>(); ++c) {
+      const int w = tid + c * NT;
+      if (w >= G * (N / R)) break;
+      const int g = w % G, bfl = w / G;
+      const int p = bfl / s, q = bfl - p * s;
+#pragma unroll
+      for (int t = 0; t < R; ++t) {
+        const int e = q + s * (p + t * m);
+        r.v[c][t] = first ? first_input(buf, kind, g, e, tb) : cb[g * LD + e];
+      }
+      Dft<T, R>::run(r.v[c]);
+      const int step = (N / n) * p;   // W_n^{p u} = root[(N/n) p u], (N/n) p u < N
+#pragma unroll
+      for (int u = 1; u < R; ++u)
+        if (p) r.v[c][u] = cmul(r.v[c][u], tb.root[step * u]);
+    }
   }
-  // spectrum is in `src`; unpack into the other buffer
-  T* out = reinterpret_cast<T*>(dst);
+
+  template <int R>
+  QHD static void stage_write(int tid, T* buf, int kind, int n, int s, bool last, const StageRegs<R>& r) {
+    Cx<T>* cb = reinterpret_cast<Cx<T>*>(buf);
+#pragma unroll
+    for (int c = 0; c < per_thread<R>(); ++c) {
+      const int w = tid + c * NT;
+      if (w >= G * (N / R)) break;
+      const int g = w % G, bfl = w / G;
+      const int p = bfl / s, q = bfl - p * s;
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        const int k = q + s * (R * p + u);
+        if (last && !is_forward(kind)) last_output_inverse(buf, kind, g, k, r.v[c][u]);
+        else cb[g * LD + k] = r.v[c][u];
+      }
+    }
+  }
+
+  // ---- forward kinds: pair Z_k with Z_{N-k} ---------------------------------
+  static constexpr int kPairs = N / 2 + 1;   // k = 0 .. N/2
+  static constexpr int kUnpackPerThread = (G * kPairs + NT - 1) / NT;
+  struct UnpackRegs {
+    T ya[kUnpackPerThread][2], yb[kUnpackPerThread][2];
+  };
+
+  QHD static void unpack_read(int tid, const T* buf, int kind, Tables<T> tb, UnpackRegs& r) {
+    const Cx<T>* cb = reinterpret_cast<const Cx<T>*>(buf);
+    (void)kind;
+#pragma unroll
+    for (int c = 0; c < kUnpackPerThread; ++c) {
+      const int w = tid + c * NT;
+      if (w >= G * kPairs) break;
+      const int g = w % G, k = w / G;
+      const int kn = (N - k) % N;
+      const Cx<T> z0 = cb[g * LD + k], z1 = cb[g * LD + kn];
+      // y(k) from (Z_k, Z_{N-k}); y(N-k) from (Z_{N-k}, Z_k)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const Cx<T> zk = h ? z1 : z0;
+        const Cx<T> zr = conj(h ? z0 : z1);
+        const int kk = h ? kn : k;
+        const Cx<T> va = zk + zr;
+        const Cx<T> d = zk - zr;
+        const Cx<T> vb = {d.y, -d.x};
+        const Cx<T> qk = tb.quarter[kk];
+        r.ya[c][h] = qk.x * va.x - qk.y * va.y;
+        r.yb[c][h] = qk.x * vb.x - qk.y * vb.y;
+      }
+    }
+  }
+
+  QHD static void unpack_write(int tid, T* buf, int kind, const UnpackRegs& r) {
+#pragma unroll
+    for (int c = 0; c < kUnpackPerThread; ++c) {
+      const int w = tid + c * NT;
+      if (w >= G * kPairs) break;
+      const int g = w % G, k = w / G;
+      T* a = buf + (2 * g) * LD;
+      T* b = a + LD;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        if (h && (k == 0 || k == N / 2)) continue;   // self-paired
+        const int kk = h ? N - k : k;
+        const int dst = kind == O10 ? N - 1 - kk : kk;
+        a[dst] = r.ya[c][h];
+        b[dst] = r.yb[c][h];
+      }
+    }
+  }
+};
+
+// Runs the whole in-place transform of the tile in `buf`.  `ex.phase2(rd, wr,
+// tid, regs)` runs rd(tid, regs), synchronises the CTA, runs wr(tid, regs) and
+// synchronises again on the device; the CPU test runs rd for every thread
+// (each with its own registers) before any wr.
+template <typename T, int N, int G, int NT, int ST, class Exec>
+QHD void r2r_stages(Exec& ex, int tid, int kind, T* buf, Tables<T> tb, int n, int s) {
+  using F = TileFFT<T, N, G, NT>;
+  if constexpr (ST < F::plan.n_stages) {
+    constexpr int R = F::plan.r[ST];
+    constexpr bool first = ST == 0, last = ST == F::plan.n_stages - 1;
+    using Regs = typename F::template StageRegs<R>;
+    Regs regs;
+    ex.phase2([&](int t, Regs& rg) { F::template stage_read<R>(t, buf, kind, n, s, first, tb, rg); },
+              [&](int t, Regs& rg) { F::template stage_write<R>(t, buf, kind, n, s, last, rg); }, tid, regs);
+    r2r_stages<T, N, G, NT, ST + 1>(ex, tid, kind, buf, tb, n / R, s * R);
+  }
+}
+
+template <typename T, int N, int G, int NT, class Exec>
+QHD void r2r_tile_inplace(Exec& ex, int tid, int kind, T* buf, Tables<T> tb) {
+  using F = TileFFT<T, N, G, NT>;
+  r2r_stages<T, N, G, NT, 0>(ex, tid, kind, buf, tb, N, 1);
   if (is_forward(kind)) {
-    ex.loop(G * N, [&](int w) { fwd_unpack<T, N>(w, G, kind, src, LD, out, LD, tb); });
-  } else {
-    ex.loop(G * (N / 2), [&](int w) { inv_unpack<T, N>(w, G, kind, src, LD, out, LD); });
+    typename F::UnpackRegs regs;
+    ex.phase2([&](int t, typename F::UnpackRegs& rg) { F::unpack_read(t, buf, kind, tb, rg); },
+              [&](int t, typename F::UnpackRegs& rg) { F::unpack_write(t, buf, kind, rg); }, tid, regs);
   }
-  return out;
 }
 
 }  // namespace quasi

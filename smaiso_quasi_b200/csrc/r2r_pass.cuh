@@ -18,12 +18,12 @@
 
 namespace quasi {
 
-constexpr int kPassThreads = 128;
-
 struct DevExec {
-  template <class F>
-  __device__ __forceinline__ void loop(int count, F&& f) {
-    for (int w = threadIdx.x; w < count; w += blockDim.x) f(w);
+  template <class R, class W, class Regs>
+  __device__ __forceinline__ void phase2(R&& rd, W&& wr, int tid, Regs& regs) {
+    rd(tid, regs);
+    __syncthreads();
+    wr(tid, regs);
     __syncthreads();
   }
 };
@@ -48,36 +48,69 @@ __device__ __forceinline__ void tile_coords(const Geom& g, int tile, int P, int 
   }
 }
 
-template <typename T, int N>
-__device__ __noinline__ T* r2r_tile_dev(int kind, int G, T* a, T* b, Tables<T> tb) {
-  DevExec ex;
-  return r2r_tile<T, N>(ex, kind, G, a, b, tb);
+// Element e of a tile -> (pencil p, position n).  z tiles are P contiguous
+// rows (n fastest); x/y tiles have P consecutive k (p fastest): either way
+// neighbouring threads touch neighbouring addresses in global memory.
+template <int AXIS, int P, int N>
+__device__ __forceinline__ void tile_elem(int e, int& p, int& n) {
+  if (AXIS == 2) { p = e / N; n = e - p * N; }
+  else { n = e / P; p = e - n * P; }
 }
 
+// Threads per CTA: one radix-R_max butterfly per thread and pencil pair.
+template <typename T> constexpr int pass_threads() { return sizeof(T) == 8 ? 128 : 256; }
+// CTAs per SM the register allocation must allow (<= 128 registers/thread).
+template <typename T> constexpr int pass_min_blocks() { return sizeof(T) == 8 ? 4 : 2; }
+
 template <typename T, int N, int AXIS, int P, class Load, class Store>
-__global__ void __launch_bounds__(kPassThreads) axis_pass_kernel(Geom g, int kind, Tables<T> tb, Load ld, Store st) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+__global__ void __launch_bounds__(pass_threads<T>(), pass_min_blocks<T>()) axis_pass_kernel(Geom g, int kind, Tables<T> tb, Load ld,
+                                                                      Store st) {
+  constexpr int NT = pass_threads<T>();
   constexpr int LD = tile_ld(N);
-  T* A = reinterpret_cast<T*>(smem_raw);
-  T* B = A + P * LD;
+  constexpr int E = P * N;
+  constexpr int PER = (E + NT - 1) / NT;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* buf = reinterpret_cast<T*>(smem_raw);
   const int tile = blockIdx.x;
-  for (int e = threadIdx.x; e < P * N; e += blockDim.x) {
-    int p, n;
-    if (AXIS == 2) { p = e / N; n = e - p * N; }
-    else { n = e / P; p = e - n * P; }
-    int i, j, k;
-    tile_coords<AXIS>(g, tile, P, p, n, i, j, k);
-    A[p * LD + n] = ld(i, j, k);
+  const int tid = threadIdx.x;
+  // loads go out in batches of B per thread (B * NT * sizeof(T) bytes in
+  // flight per CTA) before any of them is consumed
+  constexpr int B = PER < 16 ? PER : 16;
+#pragma unroll
+  for (int c0 = 0; c0 < PER; c0 += B) {
+    T v[B];
+#pragma unroll
+    for (int c = 0; c < B; ++c) {
+      const int e = tid + (c0 + c) * NT;
+      if ((E % NT == 0 && PER % B == 0) || (c0 + c < PER && e < E)) {
+        int p, n, i, j, k;
+        tile_elem<AXIS, P, N>(e, p, n);
+        tile_coords<AXIS>(g, tile, P, p, n, i, j, k);
+        v[c] = ld(i, j, k);
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < B; ++c) {
+      const int e = tid + (c0 + c) * NT;
+      if ((E % NT == 0 && PER % B == 0) || (c0 + c < PER && e < E)) {
+        int p, n;
+        tile_elem<AXIS, P, N>(e, p, n);
+        buf[p * LD + n] = v[c];
+      }
+    }
   }
   __syncthreads();
-  T* out = r2r_tile_dev<T, N>(kind, P / 2, A, B, tb);
-  for (int e = threadIdx.x; e < P * N; e += blockDim.x) {
-    int p, n;
-    if (AXIS == 2) { p = e / N; n = e - p * N; }
-    else { n = e / P; p = e - n * P; }
-    int i, j, k;
-    tile_coords<AXIS>(g, tile, P, p, n, i, j, k);
-    st(i, j, k, out[p * LD + n]);
+  DevExec ex;
+  r2r_tile_inplace<T, N, P / 2, NT>(ex, tid, kind, buf, tb);
+#pragma unroll
+  for (int c = 0; c < PER; ++c) {
+    const int e = tid + c * NT;
+    if (E % NT == 0 || e < E) {
+      int p, n, i, j, k;
+      tile_elem<AXIS, P, N>(e, p, n);
+      tile_coords<AXIS>(g, tile, P, p, n, i, j, k);
+      st(i, j, k, buf[p * LD + n]);
+    }
   }
 }
 
@@ -88,7 +121,7 @@ template <typename T> constexpr int pass_pencils(int n) {
 
 template <typename T, int N, int AXIS, int P>
 inline size_t pass_smem_bytes() {
-  return size_t(2) * P * tile_ld(N) * sizeof(T);
+  return size_t(P) * tile_ld(N) * sizeof(T);
 }
 
 template <typename T, int N, int AXIS, int P, class Load, class Store>
@@ -105,7 +138,7 @@ cudaError_t launch_pass_n(const Geom& g, int kind, Tables<T> tb, Load ld, Store 
   if (AXIS == 2) tiles = (g.nx * g.ny) / P;
   else if (AXIS == 1) tiles = g.nx * (g.nz / P);
   else tiles = g.ny * (g.nz / P);
-  kern<<<tiles, kPassThreads, smem, s>>>(g, kind, tb, ld, st);
+  kern<<<tiles, pass_threads<T>(), smem, s>>>(g, kind, tb, ld, st);
   return cudaGetLastError();
 }
 

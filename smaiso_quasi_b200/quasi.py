@@ -35,7 +35,7 @@ EXPORTS = [
     "quasi_set_psi", "quasi_init", "quasi_step", "quasi_step_timed", "quasi_step_count", "quasi_get_field",
     "quasi_diagnostics", "quasi_growth_rate", "quasi_save", "quasi_load", "quasi_r2r_plan_create",
     "quasi_r2r_execute_device", "quasi_r2r_execute_host", "quasi_r2r_plan_destroy",
-    "quasi_ic_default", "quasi_initial_condition",
+    "quasi_ic_default", "quasi_initial_condition", "quasi_step_kernels", "quasi_time_axis_pass",
 ]
 IC_KIND = {"planar": 0, "undulated": 1, "interface": 2, "droplet": 3, "stb": 4, "focal_conic": 5}
 
@@ -100,6 +100,8 @@ def lib() -> ctypes.CDLL:
         L.quasi_r2r_execute_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         L.quasi_r2r_execute_host.argtypes = [ctypes.c_void_p, dp, dp]
         L.quasi_r2r_plan_destroy.argtypes = [ctypes.c_void_p]
+        L.quasi_step_kernels.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
+        L.quasi_time_axis_pass.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, dp]
         L.quasi_ic_default.argtypes = [ctypes.POINTER(IC), ctypes.c_int]
         L.quasi_initial_condition.argtypes = [ctypes.POINTER(Config), ctypes.POINTER(IC), dp]
         _lib = L
@@ -185,6 +187,16 @@ class Simulation:
         v = ctypes.c_long()
         _check(lib().quasi_step_count(self._h, ctypes.byref(v)))
         return v.value
+
+    def step_kernels(self) -> int:
+        n = ctypes.c_int()
+        _check(lib().quasi_step_kernels(self._h, ctypes.byref(n)))
+        return n.value
+
+    def time_axis_pass(self, axis: int, reps: int = 20) -> float:
+        ms = ctypes.c_double()
+        _check(lib().quasi_time_axis_pass(self._h, int(axis), int(reps), ctypes.byref(ms)))
+        return ms.value
 
     def field(self, name: str) -> np.ndarray:
         out = np.empty(self.shape, dtype=np.float64)
