@@ -58,14 +58,20 @@ static __global__ void diag_final_kernel(const double* partial, int nblocks, dou
 template <typename T>
 class Engine : public EngineBase {
  public:
-  static constexpr int kFields = 32;
+  static constexpr int kFields = 34;
+  static constexpr int kPhases = 6;   // lcm of the 3-buffer psiq and 2-buffer Nq rotations
 
   explicit Engine(const quasi_config& cfg) : cfg_(cfg) {}
 
   ~Engine() override {
     if (dev_ok_) cudaSetDevice(cfg_.device);
-    if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
-    if (slab_) cudaFree(slab_);
+    for (auto& ge : graph_exec_)
+      if (ge) cudaGraphExecDestroy(ge);
+    if (slab_) {
+      MapCache::get().forget(slab_, static_cast<char*>(slab_) + size_t(kFields) * n_ * sizeof(T));
+      cudaFree(slab_);
+    }
+    if (tma_err_) cudaFree(tma_err_);
     if (tabs_) cudaFree(tabs_);
     if (nloop_dev_) cudaFree(nloop_dev_);
     if (partial_) cudaFree(partial_);
@@ -93,6 +99,10 @@ class Engine : public EngineBase {
     if (!cuda_ok(cudaMalloc(&nloop_dev_, sizeof(int)), "malloc") || !cuda_ok(cudaMemset(nloop_dev_, 0, sizeof(int)), "memset"))
       return QUASI_ERR_CUDA;
     if (!cuda_ok(cudaMalloc(&partial_, (kDiagBlocks * 4 + 4) * sizeof(double)), "malloc")) return QUASI_ERR_CUDA;
+    if (!cuda_ok(cudaMalloc(&tma_err_, sizeof(int)), "malloc") || !cuda_ok(cudaMemset(tma_err_, 0, sizeof(int)), "memset"))
+      return QUASI_ERR_CUDA;
+    if (!cuda_ok(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, cfg_.device), "attribute"))
+      return QUASI_ERR_CUDA;
     if (!cuda_ok(cudaMallocHost(&host_stage_, n_ * sizeof(T) + 64), "host alloc")) return QUASI_ERR_NOMEM;
     // wavenumber tables, quasi.cpp:397-431
     const int len[3] = {g_.nx, g_.ny, g_.nz};
@@ -126,6 +136,8 @@ class Engine : public EngineBase {
 
   int init() override {
     if (!have_psi_) { err = "quasi_init before quasi_set_psi"; return QUASI_ERR_STATE; }
+    set_phase(0);
+    use_tma();
     if (!cuda_ok(enqueue_init<T>(c_, tb_, nloop_dev_, stream_), "init")) return QUASI_ERR_CUDA;
     if (!cuda_ok(cudaStreamSynchronize(stream_), "init sync")) return QUASI_ERR_CUDA;
     nloop_ = 0;
@@ -136,15 +148,19 @@ class Engine : public EngineBase {
   int step(int nsteps, double* device_ms) override {
     if (!initialized_) { err = "quasi_step before quasi_init"; return QUASI_ERR_STATE; }
     if (nsteps < 0) { err = "nsteps < 0"; return QUASI_ERR_INVALID; }
-    if (!graph_exec_) {
+    if (!graph_exec_[0]) {
       int rc = capture();
       if (rc) return rc;
     }
     if (device_ms && !cuda_ok(cudaEventRecord(ev0_, stream_), "event")) return QUASI_ERR_CUDA;
     for (int s = 0; s < nsteps; ++s)
-      if (!cuda_ok(cudaGraphLaunch(graph_exec_, stream_), "graph launch")) return QUASI_ERR_CUDA;
+      if (!cuda_ok(cudaGraphLaunch(graph_exec_[(nloop_ + s) % kPhases], stream_), "graph launch"))
+        return QUASI_ERR_CUDA;
     if (device_ms && !cuda_ok(cudaEventRecord(ev1_, stream_), "event")) return QUASI_ERR_CUDA;
     if (!cuda_ok(cudaStreamSynchronize(stream_), "step sync")) return QUASI_ERR_CUDA;
+    int tma_failed = 0;
+    if (!cuda_ok(cudaMemcpy(&tma_failed, tma_err_, sizeof(int), cudaMemcpyDeviceToHost), "flag")) return QUASI_ERR_CUDA;
+    if (tma_failed) { err = "a tile copy did not complete within its wait limit"; return QUASI_ERR_CUDA; }
     if (device_ms) {
       float ms = 0;
       if (!cuda_ok(cudaEventElapsedTime(&ms, ev0_, ev1_), "elapsed")) return QUASI_ERR_CUDA;
@@ -155,6 +171,7 @@ class Engine : public EngineBase {
   }
 
   int get_field(int field, double* host) override {
+    set_phase(nloop_);
     const T* src = field_ptr(field);
     if (!src) { err = "unknown or unavailable field " + std::to_string(field); return QUASI_ERR_INVALID; }
     T* st = static_cast<T*>(host_stage_);
@@ -187,6 +204,7 @@ class Engine : public EngineBase {
     if (i < 0 || i >= g_.nx || k < 0 || k >= g_.nz) { err = "growth probe mode outside the grid"; return QUASI_ERR_INVALID; }
     const size_t id = (size_t(i) * g_.ny + 0) * g_.nz + k;
     T a, b;
+    set_phase(nloop_);
     if (!cuda_ok(cudaMemcpyAsync(&a, c_.psiq + id, sizeof(T), cudaMemcpyDeviceToHost, stream_), "D2H") ||
         !cuda_ok(cudaMemcpyAsync(&b, c_.psiq_old + id, sizeof(T), cudaMemcpyDeviceToHost, stream_), "D2H") ||
         !cuda_ok(cudaStreamSynchronize(stream_), "sync"))
@@ -202,6 +220,7 @@ class Engine : public EngineBase {
     if (!f) { err = std::string("cannot open ") + path; return QUASI_ERR_IO; }
     Header hd = header();
     f.write(reinterpret_cast<const char*>(&hd), sizeof(hd));
+    set_phase(nloop_);
     for (T* p : carried()) {
       if (!cuda_ok(cudaMemcpy(host_stage_, p, n_ * sizeof(T), cudaMemcpyDeviceToHost), "D2H")) return QUASI_ERR_CUDA;
       f.write(static_cast<const char*>(host_stage_), n_ * sizeof(T));
@@ -221,6 +240,7 @@ class Engine : public EngineBase {
       err = "checkpoint grid/variant/precision does not match the handle";
       return QUASI_ERR_IO;
     }
+    set_phase(hd.nloop);
     for (T* p : carried()) {
       f.read(static_cast<char*>(host_stage_), n_ * sizeof(T));
       if (!f) { err = "checkpoint is truncated"; return QUASI_ERR_IO; }
@@ -236,7 +256,7 @@ class Engine : public EngineBase {
   long nloop() const override { return nloop_; }
 
   int step_kernels(int* n) override {
-    if (!graph_exec_) {
+    if (!graph_exec_[0]) {
       if (!initialized_) { err = "step graph not captured yet (call quasi_init)"; return QUASI_ERR_STATE; }
       int rc = capture();
       if (rc) return rc;
@@ -248,6 +268,7 @@ class Engine : public EngineBase {
   int time_axis_pass(int axis, int reps, double* avg_ms) override {
     if (axis < 0 || axis > 2 || reps < 1) { err = "axis must be 0..2 and reps >= 1"; return QUASI_ERR_INVALID; }
     T* d = c_.tmp;
+    use_tma();
     auto one = [&]() -> cudaError_t {
       if (axis == 0) return launch_pass<T, 0>(g_, E01, tb_.t[0], LoadField<T>{g_, d}, StoreField<T>{g_, d}, stream_);
       if (axis == 1) return launch_pass<T, 1>(g_, E01, tb_.t[1], LoadField<T>{g_, d}, StoreField<T>{g_, d}, stream_);
@@ -278,9 +299,28 @@ class Engine : public EngineBase {
     h.nloop = nloop_;
     return h;
   }
+  // the state a step reads (at the phase set by set_phase(nloop))
   std::vector<T*> carried() {
-    return {c_.psiq, c_.psiq_old, c_.Nq, c_.Nq_old, c_.rhoq, c_.rho_old, c_.rho, c_.vx, c_.vy, c_.vz,
+    return {c_.psiq, c_.psiq_old, c_.Nq_old, c_.rhoq, c_.rho_old, c_.rho, c_.vx, c_.vy, c_.vz,
             c_.divv, c_.divvq, c_.psi, c_.psi_old, c_.p, c_.df};
+  }
+
+  // Buffer rotation for a step that starts after `s` completed steps:
+  // psiq = A[s%3], psiq_old = A[(s+2)%3], psiq_new = A[(s+1)%3];
+  // Nq (computed this step) = B[s%2], Nq_old = B[(s+1)%2].
+  void set_phase(long s) {
+    c_.psiq = psiq_buf_[s % 3];
+    c_.psiq_old = psiq_buf_[(s + 2) % 3];
+    c_.psiq_new = psiq_buf_[(s + 1) % 3];
+    c_.Nq = nq_buf_[s % 2];
+    c_.Nq_old = nq_buf_[(s + 1) % 2];
+  }
+
+  void use_tma() {
+    TmaConfig& t = tma_config();
+    t.err = tma_err_;
+    t.sms = sms_;
+    t.enabled = true;
   }
 
   bool cuda_ok(cudaError_t e, const char* what) {
@@ -311,7 +351,10 @@ class Engine : public EngineBase {
     c_.n0 = g_.nx / (cfg_.emulate_ranks > 0 ? cfg_.emulate_ranks : 1);
     c_.nloop = nloop_dev_;
     c_.store_dtpsi = quasi ? 0 : 1;
-    c_.psiq = next(); c_.psiq_old = next(); c_.Nq = next(); c_.Nq_old = next(); c_.rhoq = next();
+    for (auto& b : psiq_buf_) b = next();
+    for (auto& b : nq_buf_) b = next();
+    set_phase(0);
+    c_.rhoq = next();
     c_.divvq = next(); c_.Sx = next(); c_.Sy = next(); c_.Sz = next();
     c_.psi = next(); c_.psi_old = next(); c_.rho = next(); c_.rho_old = next();
     c_.vx = next(); c_.vy = next(); c_.vz = next(); c_.divv = next(); c_.p = next();
@@ -338,7 +381,18 @@ class Engine : public EngineBase {
   }
 
   int capture() {
+    for (int ph = 0; ph < kPhases; ++ph) {
+      int rc = capture_phase(ph);
+      if (rc) return rc;
+    }
+    set_phase(nloop_);
+    return QUASI_OK;
+  }
+
+  int capture_phase(int ph) {
     cudaGraph_t graph = nullptr;
+    set_phase(ph);
+    use_tma();
     if (!cuda_ok(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture"))
       return QUASI_ERR_CUDA;
     cudaError_t e = enqueue_step<T>(c_, tb_, nloop_dev_, stream_);
@@ -356,9 +410,9 @@ class Engine : public EngineBase {
       cudaGraphNodeType t;
       if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++graph_kernels_;
     }
-    e = cudaGraphInstantiate(&graph_exec_, graph, 0);
+    e = cudaGraphInstantiate(&graph_exec_[ph], graph, 0);
     cudaGraphDestroy(graph);
-    if (!cuda_ok(e, "graph instantiate")) { graph_exec_ = nullptr; return QUASI_ERR_CUDA; }
+    if (!cuda_ok(e, "graph instantiate")) { graph_exec_[ph] = nullptr; return QUASI_ERR_CUDA; }
     return QUASI_OK;
   }
 
@@ -372,11 +426,15 @@ class Engine : public EngineBase {
   double* tabs_ = nullptr;
   int* nloop_dev_ = nullptr;
   double* partial_ = nullptr;
+  int* tma_err_ = nullptr;
+  int sms_ = 148;
   void* host_stage_ = nullptr;
   DevTwiddles<T> tw_[3];
   AxisTables<T> tb_{};
   StepCtx<T> c_{};
-  cudaGraphExec_t graph_exec_ = nullptr;
+  cudaGraphExec_t graph_exec_[kPhases] = {};
+  T* psiq_buf_[3] = {};
+  T* nq_buf_[2] = {};
   int graph_kernels_ = 0;
   long nloop_ = 0;
 };

@@ -15,6 +15,14 @@ struct R2RBase {
   virtual cudaError_t exec(void* data, cudaStream_t s) = 0;
   int nx, ny, nz, device, elem;
   cudaStream_t own = nullptr;
+  int* tma_err = nullptr;
+  int sms = 148;
+  void use_tma() {
+    TmaConfig& t = tma_config();
+    t.err = tma_err;
+    t.sms = sms;
+    t.enabled = true;
+  }
 };
 
 template <typename T>
@@ -26,6 +34,7 @@ struct R2R : R2RBase {
     cudaSetDevice(device);
     for (auto& t : tw) t.release();
     if (own) cudaStreamDestroy(own);
+    if (tma_err) cudaFree(tma_err);
   }
   cudaError_t setup() {
     const int len[3] = {nx, ny, nz};
@@ -34,12 +43,16 @@ struct R2R : R2RBase {
       if ((e = tw[a].upload(len[a])) != cudaSuccess) return e;
       tb.t[a] = tw[a].tables();
     }
+    if ((e = cudaMalloc(&tma_err, sizeof(int))) != cudaSuccess) return e;
+    if ((e = cudaMemset(tma_err, 0, sizeof(int))) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess) return e;
     return cudaStreamCreateWithFlags(&own, cudaStreamNonBlocking);
   }
   cudaError_t exec(void* data, cudaStream_t s) override {
     T* d = static_cast<T*>(data);
     const Geom g{nx, ny, nz};
     cudaError_t e;
+    use_tma();
     if ((e = launch_pass<T, 2>(g, kind[2], tb.t[2], LoadField<T>{g, d}, StoreField<T>{g, d}, s)) != cudaSuccess)
       return e;
     if ((e = launch_pass<T, 1>(g, kind[1], tb.t[1], LoadField<T>{g, d}, StoreField<T>{g, d}, s)) != cudaSuccess)
@@ -137,6 +150,7 @@ int quasi_r2r_execute_host(quasi_r2r_plan* p, const double* in, double* out) {
     else e = cudaMemcpyAsync(f.data(), d, n * 4, cudaMemcpyDeviceToHost, b->own);
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(b->own);
+  quasi::MapCache::get().forget(d, static_cast<char*>(d) + n * b->elem);
   cudaFree(d);
   if (e != cudaSuccess) return set_error(QUASI_ERR_CUDA, cudaGetErrorString(e));
   if (b->elem == 4)

@@ -164,22 +164,47 @@ struct Tables {
 };
 
 // ---------------------------------------------------------------------------
-// In-place tile transform.
+// Tile transform with pluggable input and output.
 //
-// Tile: P = 2G real pencils of length N at buf[r * LD + n] (reals), LD = N + 1.
-// Complex pencil g (LD complex elements) occupies exactly the bytes of real
-// pencils 2g and 2g+1, so the whole transform runs in ONE buffer: every stage
-// reads all its inputs into registers, the CTA synchronises, then writes.
+// G complex pencils of length N live in a shared buffer `cb` (pencil g at
+// cb[g * LD + e], LD = N + 1) between stages.  Complex pencil g carries the
+// real pencils 2g (real part) and 2g+1 (imaginary part).
+//   Src::pair(g, n, a, b)  the two reals of pencils 2g, 2g+1 at position n
+//   Snk::put(g, n, a, b)   store the two reals of pencils 2g, 2g+1 at n
+// The first stage reads through Src with the Makhoul reordering folded in;
+// the last stage of an inverse kind writes through Snk with the
+// un-reordering folded in; a forward kind pairs Z_k with Z_{N-k} from the
+// shared buffer and writes through Snk.  When Src/Snk are the shared buffer
+// itself (in-place, real pencil r at r * LD) every read half is separated
+// from its write half by a barrier; when they are global memory the first
+// stage needs no barrier before its shared writes and an inverse kind's last
+// stage none before its global stores.
+//
 // Work items are mapped pencil-fastest (g = w % G) so that neighbouring
-// threads touch the same offset of neighbouring pencils; the odd stride LD
-// keeps those in distinct shared-memory banks.
-//
-// The Makhoul reordering is folded into the first stage's reads (forward
-// kinds, and the inverse kinds' V_k = e^{i pi k/2N}(y_k - i y_{N-k})) and the
-// inverse un-reordering into the last stage's writes; the forward kinds'
-// pairing of Z_k with Z_{N-k} is one extra read/write phase.
+// threads touch the same offset of neighbouring pencils: conflict-free with
+// the odd stride LD in shared memory and coalesced (adjacent k) in global.
 // ---------------------------------------------------------------------------
 QHD constexpr int tile_ld(int n) { return n + 1; }
+
+template <typename T>
+struct SmemSrc {
+  const T* buf;
+  int ld;
+  QHD void pair(int g, int n, T& a, T& b) const {
+    a = buf[(2 * g) * ld + n];
+    b = buf[(2 * g + 1) * ld + n];
+  }
+};
+
+template <typename T>
+struct SmemSnk {
+  T* buf;
+  int ld;
+  QHD void put(int g, int n, T a, T b) const {
+    buf[(2 * g) * ld + n] = a;
+    buf[(2 * g + 1) * ld + n] = b;
+  }
+};
 
 template <typename T, int N, int G, int NT>
 struct TileFFT {
@@ -189,33 +214,27 @@ struct TileFFT {
 
   // butterflies a thread owns in a radix-R stage
   template <int R> static constexpr int per_thread() { return (G * (N / R) + NT - 1) / NT; }
-  static constexpr int kMaxRegs = 16;   // complex values a thread holds in any phase
 
-  // ---- stage input element e of complex pencil g --------------------------
-  // first stage: the packed complex sequence is formed from the real tile
-  QHD static Cx<T> first_input(const T* buf, int kind, int g, int e, Tables<T> tb) {
-    const T* a = buf + (2 * g) * LD;
-    const T* b = a + LD;
+  // first stage: the packed complex input e of pencil g, formed from Src
+  template <class Src>
+  QHD static Cx<T> first_input(const Src& src, int kind, int g, int e, Tables<T> tb) {
     if (is_forward(kind)) {
       // v_e = x_{2e} (e < N/2), x_{2(N-1-e)+1} (e >= N/2); DST-II negates odd x
-      int src;
+      int n;
       T sgn = T(1);
-      if (e < N / 2) src = 2 * e;
-      else { src = 2 * (N - 1 - e) + 1; if (kind == O10) sgn = T(-1); }
-      return Cx<T>{sgn * a[src], sgn * b[src]};
+      if (e < N / 2) n = 2 * e;
+      else { n = 2 * (N - 1 - e) + 1; if (kind == O10) sgn = T(-1); }
+      T a, b;
+      src.pair(g, n, a, b);
+      return Cx<T>{sgn * a, sgn * b};
     }
     // inverse: conj( e^{+i pi k/2N} [(ya_k - i ya_{N-k}) + i (yb_k - i yb_{N-k})] ), y_N = 0,
     // input reversed for DST-III
     const int k = e;
     const bool rev = kind == O01;
-    const int ik = rev ? N - 1 - k : k;
-    const T ak = a[ik], bk = b[ik];
-    T an = T(0), bn = T(0);
-    if (k) {
-      const int in_ = rev ? k - 1 : N - k;   // index of y_{N-k} (reversed: N-1-(N-k))
-      an = a[in_];
-      bn = b[in_];
-    }
+    T ak, bk, an = T(0), bn = T(0);
+    src.pair(g, rev ? N - 1 - k : k, ak, bk);
+    if (k) src.pair(g, rev ? k - 1 : N - k, an, bn);
     const Cx<T> q = tb.quarter[k];
     const Cx<T> ec = {q.x, -q.y};
     const Cx<T> va = cmul(ec, Cx<T>{ak, -an});
@@ -223,29 +242,14 @@ struct TileFFT {
     return Cx<T>{va.x - vb.y, -(va.y + vb.x)};
   }
 
-  // last stage of an inverse kind: FFT output F_k -> u_k = conj(F_k) -> the
-  // two real pencils at the un-reordered positions (DST-III negates odd x)
-  QHD static void last_output_inverse(T* buf, int kind, int g, int k, Cx<T> f) {
-    T* a = buf + (2 * g) * LD;
-    T* b = a + LD;
-    int dst;
-    T sgn = T(1);
-    if (k < N / 2) dst = 2 * k;
-    else { dst = 2 * (N - 1 - k) + 1; if (kind == O01) sgn = T(-1); }
-    a[dst] = sgn * f.x;
-    b[dst] = -sgn * f.y;
-  }
-
-  // ---- one Stockham stage, split into its read and write halves -----------
   template <int R>
   struct StageRegs {
     Cx<T> v[per_thread<R>()][R];
   };
 
-  template <int R>
-  QHD static void stage_read(int tid, const T* buf, int kind, int n, int s, bool first, Tables<T> tb,
-                             StageRegs<R>& r) {
-    const Cx<T>* cb = reinterpret_cast<const Cx<T>*>(buf);
+  template <int R, class Src>
+  QHD static void stage_read(int tid, const Cx<T>* cb, const Src& src, int kind, int n, int s, bool first,
+                             Tables<T> tb, StageRegs<R>& r) {
     const int m = n / R;
 #pragma unroll
     for (int c = 0; c < per_thread<R>(); ++c) {
@@ -256,7 +260,7 @@ struct TileFFT {
 #pragma unroll
       for (int t = 0; t < R; ++t) {
         const int e = q + s * (p + t * m);
-        r.v[c][t] = first ? first_input(buf, kind, g, e, tb) : cb[g * LD + e];
+        r.v[c][t] = first ? first_input(src, kind, g, e, tb) : cb[g * LD + e];
       }
       Dft<T, R>::run(r.v[c]);
       const int step = (N / n) * p;   // W_n^{p u} = root[(N/n) p u], (N/n) p u < N
@@ -266,9 +270,9 @@ struct TileFFT {
     }
   }
 
-  template <int R>
-  QHD static void stage_write(int tid, T* buf, int kind, int n, int s, bool last, const StageRegs<R>& r) {
-    Cx<T>* cb = reinterpret_cast<Cx<T>*>(buf);
+  template <int R, class Snk>
+  QHD static void stage_write(int tid, Cx<T>* cb, const Snk& snk, int kind, int s, bool last,
+                              const StageRegs<R>& r) {
 #pragma unroll
     for (int c = 0; c < per_thread<R>(); ++c) {
       const int w = tid + c * NT;
@@ -278,22 +282,29 @@ struct TileFFT {
 #pragma unroll
       for (int u = 0; u < R; ++u) {
         const int k = q + s * (R * p + u);
-        if (last && !is_forward(kind)) last_output_inverse(buf, kind, g, k, r.v[c][u]);
-        else cb[g * LD + k] = r.v[c][u];
+        const Cx<T> f = r.v[c][u];
+        if (last && !is_forward(kind)) {
+          // u_k = conj(F_k) -> x_{2k} (k < N/2) or x_{2(N-1-k)+1}; DST-III negates odd x
+          int n;
+          T sgn = T(1);
+          if (k < N / 2) n = 2 * k;
+          else { n = 2 * (N - 1 - k) + 1; if (kind == O01) sgn = T(-1); }
+          snk.put(g, n, sgn * f.x, -sgn * f.y);
+        } else {
+          cb[g * LD + k] = f;
+        }
       }
     }
   }
 
-  // ---- forward kinds: pair Z_k with Z_{N-k} ---------------------------------
-  static constexpr int kPairs = N / 2 + 1;   // k = 0 .. N/2
+  // forward kinds: y(k) and y(N-k) from the pair (Z_k, Z_{N-k}), k = 0..N/2
+  static constexpr int kPairs = N / 2 + 1;
   static constexpr int kUnpackPerThread = (G * kPairs + NT - 1) / NT;
   struct UnpackRegs {
     T ya[kUnpackPerThread][2], yb[kUnpackPerThread][2];
   };
 
-  QHD static void unpack_read(int tid, const T* buf, int kind, Tables<T> tb, UnpackRegs& r) {
-    const Cx<T>* cb = reinterpret_cast<const Cx<T>*>(buf);
-    (void)kind;
+  QHD static void unpack_read(int tid, const Cx<T>* cb, Tables<T> tb, UnpackRegs& r) {
 #pragma unroll
     for (int c = 0; c < kUnpackPerThread; ++c) {
       const int w = tid + c * NT;
@@ -301,69 +312,96 @@ struct TileFFT {
       const int g = w % G, k = w / G;
       const int kn = (N - k) % N;
       const Cx<T> z0 = cb[g * LD + k], z1 = cb[g * LD + kn];
-      // y(k) from (Z_k, Z_{N-k}); y(N-k) from (Z_{N-k}, Z_k)
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const Cx<T> zk = h ? z1 : z0;
         const Cx<T> zr = conj(h ? z0 : z1);
         const int kk = h ? kn : k;
-        const Cx<T> va = zk + zr;
+        const Cx<T> va = zk + zr;            // 2 V_a
         const Cx<T> d = zk - zr;
-        const Cx<T> vb = {d.y, -d.x};
-        const Cx<T> qk = tb.quarter[kk];
+        const Cx<T> vb = {d.y, -d.x};        // 2 V_b
+        const Cx<T> qk = tb.quarter[kk];     // y = 2 Re(quarter_k V)
         r.ya[c][h] = qk.x * va.x - qk.y * va.y;
         r.yb[c][h] = qk.x * vb.x - qk.y * vb.y;
       }
     }
   }
 
-  QHD static void unpack_write(int tid, T* buf, int kind, const UnpackRegs& r) {
+  template <class Snk>
+  QHD static void unpack_write(int tid, const Snk& snk, int kind, const UnpackRegs& r) {
 #pragma unroll
     for (int c = 0; c < kUnpackPerThread; ++c) {
       const int w = tid + c * NT;
       if (w >= G * kPairs) break;
       const int g = w % G, k = w / G;
-      T* a = buf + (2 * g) * LD;
-      T* b = a + LD;
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         if (h && (k == 0 || k == N / 2)) continue;   // self-paired
         const int kk = h ? N - k : k;
-        const int dst = kind == O10 ? N - 1 - kk : kk;
-        a[dst] = r.ya[c][h];
-        b[dst] = r.yb[c][h];
+        snk.put(g, kind == O10 ? N - 1 - kk : kk, r.ya[c][h], r.yb[c][h]);
       }
     }
   }
 };
 
-// Runs the whole in-place transform of the tile in `buf`.  `ex.phase2(rd, wr,
-// tid, regs)` runs rd(tid, regs), synchronises the CTA, runs wr(tid, regs) and
-// synchronises again on the device; the CPU test runs rd for every thread
-// (each with its own registers) before any wr.
-template <typename T, int N, int G, int NT, int ST, class Exec>
-QHD void r2r_stages(Exec& ex, int tid, int kind, T* buf, Tables<T> tb, int n, int s) {
+// Stage recursion.  `ex.phase(rd, wr, tid, regs, mid, after)` runs rd(tid,
+// regs), a barrier when `mid`, wr(tid, regs), a barrier when `after`; the CPU
+// test runs rd for every thread before any wr.
+struct NoHook {
+  QHD void operator()() const {}
+};
+
+// `hook()` runs on every thread right after the first stage's closing barrier
+// (the moment the first stage's input is no longer needed).
+template <typename T, int N, int G, int NT, int ST, bool INPLACE, class Exec, class Src, class Snk, class Hook>
+QHD void r2r_stages(Exec& ex, int tid, int kind, Cx<T>* cb, const Src& src, const Snk& snk, Tables<T> tb, int n,
+                    int s, const Hook& hook) {
   using F = TileFFT<T, N, G, NT>;
   if constexpr (ST < F::plan.n_stages) {
     constexpr int R = F::plan.r[ST];
     constexpr bool first = ST == 0, last = ST == F::plan.n_stages - 1;
     using Regs = typename F::template StageRegs<R>;
     Regs regs;
-    ex.phase2([&](int t, Regs& rg) { F::template stage_read<R>(t, buf, kind, n, s, first, tb, rg); },
-              [&](int t, Regs& rg) { F::template stage_write<R>(t, buf, kind, n, s, last, rg); }, tid, regs);
-    r2r_stages<T, N, G, NT, ST + 1>(ex, tid, kind, buf, tb, n / R, s * R);
+    // a read half must finish before its write half only if the writes can
+    // land on data other threads still read: always when Src/Snk are the
+    // shared buffer; otherwise only for middle stages and a forward kind's
+    // last stage (both write the shared buffer they read)
+    const bool global_out = last && !is_forward(kind);
+    const bool mid = INPLACE || (!first && !global_out);
+    // a write half must be visible before the next read half; an inverse
+    // kind's last stage writing to global memory is followed by nothing
+    const bool after = !last || is_forward(kind) || INPLACE;
+    ex.phase([&](int t, Regs& rg) { F::template stage_read<R>(t, cb, src, kind, n, s, first, tb, rg); },
+             [&](int t, Regs& rg) { F::template stage_write<R>(t, cb, snk, kind, s, last, rg); }, tid, regs, mid,
+             after);
+    if constexpr (first) {
+      if (!after) ex.sync();   // the hook may recycle the first stage's input
+      hook();
+    }
+    r2r_stages<T, N, G, NT, ST + 1, INPLACE>(ex, tid, kind, cb, src, snk, tb, n / R, s * R, hook);
   }
 }
 
-template <typename T, int N, int G, int NT, class Exec>
-QHD void r2r_tile_inplace(Exec& ex, int tid, int kind, T* buf, Tables<T> tb) {
+template <typename T, int N, int G, int NT, bool INPLACE, class Exec, class Src, class Snk, class Hook = NoHook>
+QHD void r2r_tile(Exec& ex, int tid, int kind, Cx<T>* cb, const Src& src, const Snk& snk, Tables<T> tb,
+                  const Hook& hook = Hook()) {
   using F = TileFFT<T, N, G, NT>;
-  r2r_stages<T, N, G, NT, 0>(ex, tid, kind, buf, tb, N, 1);
+  r2r_stages<T, N, G, NT, 0, INPLACE>(ex, tid, kind, cb, src, snk, tb, N, 1, hook);
   if (is_forward(kind)) {
     typename F::UnpackRegs regs;
-    ex.phase2([&](int t, typename F::UnpackRegs& rg) { F::unpack_read(t, buf, kind, tb, rg); },
-              [&](int t, typename F::UnpackRegs& rg) { F::unpack_write(t, buf, kind, rg); }, tid, regs);
+    ex.phase([&](int t, typename F::UnpackRegs& rg) { F::unpack_read(t, cb, tb, rg); },
+             [&](int t, typename F::UnpackRegs& rg) { F::unpack_write(t, snk, kind, rg); }, tid, regs, INPLACE,
+             INPLACE);
   }
+}
+
+// In-place transform of P = 2G real pencils held in `buf` (real pencil r at
+// buf[r * LD + n]); the complex pencils overlay the same bytes.
+template <typename T, int N, int G, int NT, class Exec>
+QHD void r2r_tile_inplace(Exec& ex, int tid, int kind, T* buf, Tables<T> tb) {
+  constexpr int LD = tile_ld(N);
+  r2r_tile<T, N, G, NT, true>(ex, tid, kind, reinterpret_cast<Cx<T>*>(buf), SmemSrc<T>{buf, LD}, SmemSnk<T>{buf, LD},
+                              tb);
 }
 
 }  // namespace quasi

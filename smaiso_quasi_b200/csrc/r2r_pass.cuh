@@ -14,23 +14,73 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "r2r_core.cuh"
+#include "tma.cuh"
 
 namespace quasi {
 
+template <typename T> struct Vec2;
+template <> struct Vec2<float> { using type = float2; };
+template <> struct Vec2<double> { using type = double2; };
+
 struct DevExec {
   template <class R, class W, class Regs>
-  __device__ __forceinline__ void phase2(R&& rd, W&& wr, int tid, Regs& regs) {
+  __device__ __forceinline__ void phase(R&& rd, W&& wr, int tid, Regs& regs, bool mid, bool after) {
     rd(tid, regs);
-    __syncthreads();
+    if (mid) __syncthreads();
     wr(tid, regs);
-    __syncthreads();
+    if (after) __syncthreads();
   }
+  __device__ __forceinline__ void sync() { __syncthreads(); }
 };
 
 struct Geom {
   int nx, ny, nz;
 };
+
+// ---------------------------------------------------------------------------
+// Plain loaders / storers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ size_t lin(const Geom& g, int i, int j, int k) {
+  return (size_t(i) * g.ny + j) * g.nz + k;
+}
+
+template <typename T>
+struct LoadField {
+  Geom g;
+  const T* src;
+  __device__ T operator()(int i, int j, int k) const { return src[lin(g, i, j, k)]; }
+  // k even: one aligned vector load of (k, k+1)
+  __device__ void pair(int i, int j, int k, T& a, T& b) const {
+    const auto v = *reinterpret_cast<const typename Vec2<T>::type*>(src + lin(g, i, j, k));
+    a = v.x;
+    b = v.y;
+  }
+};
+
+template <typename T>
+struct StoreField {
+  Geom g;
+  T* dst;
+  __device__ void operator()(int i, int j, int k, T v) const { dst[lin(g, i, j, k)] = v; }
+  __device__ void pair(int i, int j, int k, T a, T b) const {
+    typename Vec2<T>::type v;
+    v.x = a;
+    v.y = b;
+    *reinterpret_cast<typename Vec2<T>::type*>(dst + lin(g, i, j, k)) = v;
+  }
+};
+
+template <typename T>
+struct ScaleStore {
+  Geom g;
+  T* dst;
+  T s;
+  __device__ void operator()(int i, int j, int k, T v) const { dst[lin(g, i, j, k)] = v * s; }
+};
+
 
 template <int AXIS>
 __device__ __forceinline__ void tile_coords(const Geom& g, int tile, int P, int p, int n, int& i, int& j, int& k) {
@@ -48,18 +98,56 @@ __device__ __forceinline__ void tile_coords(const Geom& g, int tile, int P, int 
   }
 }
 
-// Element e of a tile -> (pencil p, position n).  z tiles are P contiguous
-// rows (n fastest); x/y tiles have P consecutive k (p fastest): either way
-// neighbouring threads touch neighbouring addresses in global memory.
-template <int AXIS, int P, int N>
-__device__ __forceinline__ void tile_elem(int e, int& p, int& n) {
-  if (AXIS == 2) { p = e / N; n = e - p * N; }
-  else { n = e / P; p = e - n * P; }
+// Element e of a z tile -> (pencil p, position n), n fastest (contiguous rows).
+template <int P, int N>
+__device__ __forceinline__ void z_elem(int e, int& p, int& n) {
+  p = e / N;
+  n = e - p * N;
 }
 
-// Threads per CTA: one radix-R_max butterfly per thread and pencil pair.
+// Paired access to k and k+1 (k even): the two real pencils of one complex
+// pencil in an x or y tile.  Loaders/storers may provide pair() themselves
+// (vector access); otherwise the element operator is called twice.
+template <class L, class = void> struct HasPair : std::false_type {};
+template <class L> struct HasPair<L, std::void_t<decltype(&L::pair)>> : std::true_type {};
+
+template <typename T, class Load>
+__device__ __forceinline__ void load_pair(const Load& ld, int i, int j, int k, T& a, T& b) {
+  if constexpr (HasPair<Load>::value) ld.pair(i, j, k, a, b);
+  else { a = ld(i, j, k); b = ld(i, j, k + 1); }
+}
+
+template <typename T, class Store>
+__device__ __forceinline__ void store_pair(const Store& st, int i, int j, int k, T a, T b) {
+  if constexpr (HasPair<Store>::value) st.pair(i, j, k, a, b);
+  else { st(i, j, k, a); st(i, j, k + 1, b); }
+}
+
+// x/y tiles read and write global memory directly from the FFT stages
+template <typename T, int AXIS, class Load>
+struct GlobSrc {
+  Load ld;
+  int outer, k0;
+  __device__ __forceinline__ void pair(int g, int n, T& a, T& b) const {
+    const int k = k0 + 2 * g;
+    if (AXIS == 1) load_pair<T>(ld, outer, n, k, a, b);
+    else load_pair<T>(ld, n, outer, k, a, b);
+  }
+};
+
+template <typename T, int AXIS, class Store>
+struct GlobSnk {
+  Store st;
+  int outer, k0;
+  __device__ __forceinline__ void put(int g, int n, T a, T b) const {
+    const int k = k0 + 2 * g;
+    if (AXIS == 1) store_pair<T>(st, outer, n, k, a, b);
+    else store_pair<T>(st, n, outer, k, a, b);
+  }
+};
+
+// Threads per CTA and the CTAs per SM the register allocation must allow.
 template <typename T> constexpr int pass_threads() { return sizeof(T) == 8 ? 128 : 256; }
-// CTAs per SM the register allocation must allow (<= 128 registers/thread).
 template <typename T> constexpr int pass_min_blocks() { return sizeof(T) == 8 ? 4 : 2; }
 
 template <typename T, int N, int AXIS, int P, class Load, class Store>
@@ -67,51 +155,193 @@ __global__ void __launch_bounds__(pass_threads<T>(), pass_min_blocks<T>()) axis_
                                                                       Store st) {
   constexpr int NT = pass_threads<T>();
   constexpr int LD = tile_ld(N);
-  constexpr int E = P * N;
-  constexpr int PER = (E + NT - 1) / NT;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* buf = reinterpret_cast<T*>(smem_raw);
   const int tile = blockIdx.x;
   const int tid = threadIdx.x;
-  // loads go out in batches of B per thread (B * NT * sizeof(T) bytes in
-  // flight per CTA) before any of them is consumed
-  constexpr int B = PER < 16 ? PER : 16;
+  DevExec ex;
+  if constexpr (AXIS != 2) {
+    // x / y: P consecutive k columns; first stage loads from global, an inverse
+    // kind's last stage (or a forward kind's unpack) stores to global
+    const int kt = g.nz / P;
+    const int outer = tile / kt, k0 = (tile - outer * kt) * P;
+    r2r_tile<T, N, P / 2, NT, false>(ex, tid, kind, reinterpret_cast<Cx<T>*>(buf),
+                                      GlobSrc<T, AXIS, Load>{ld, outer, k0}, GlobSnk<T, AXIS, Store>{st, outer, k0}, tb);
+  } else {
+    // z: P contiguous rows staged through shared memory (coalesced both ways)
+    constexpr int E = P * N;
+    constexpr int PER = (E + NT - 1) / NT;
+    constexpr int B = PER < 16 ? PER : 16;
 #pragma unroll
-  for (int c0 = 0; c0 < PER; c0 += B) {
-    T v[B];
+    for (int c0 = 0; c0 < PER; c0 += B) {
+      T v[B];
 #pragma unroll
-    for (int c = 0; c < B; ++c) {
-      const int e = tid + (c0 + c) * NT;
-      if ((E % NT == 0 && PER % B == 0) || (c0 + c < PER && e < E)) {
+      for (int c = 0; c < B; ++c) {
+        const int e = tid + (c0 + c) * NT;
+        if ((E % NT == 0 && PER % B == 0) || (c0 + c < PER && e < E)) {
+          int p, n, i, j, k;
+          z_elem<P, N>(e, p, n);
+          tile_coords<2>(g, tile, P, p, n, i, j, k);
+          v[c] = ld(i, j, k);
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < B; ++c) {
+        const int e = tid + (c0 + c) * NT;
+        if ((E % NT == 0 && PER % B == 0) || (c0 + c < PER && e < E)) {
+          int p, n;
+          z_elem<P, N>(e, p, n);
+          buf[p * LD + n] = v[c];
+        }
+      }
+    }
+    __syncthreads();
+    r2r_tile_inplace<T, N, P / 2, NT>(ex, tid, kind, buf, tb);
+#pragma unroll
+    for (int c = 0; c < PER; ++c) {
+      const int e = tid + c * NT;
+      if (E % NT == 0 || e < E) {
         int p, n, i, j, k;
-        tile_elem<AXIS, P, N>(e, p, n);
-        tile_coords<AXIS>(g, tile, P, p, n, i, j, k);
-        v[c] = ld(i, j, k);
+        z_elem<P, N>(e, p, n);
+        tile_coords<2>(g, tile, P, p, n, i, j, k);
+        st(i, j, k, buf[p * LD + n]);
       }
     }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Persistent TMA-pipelined pass for plain field loads.
+//
+// Each CTA walks tiles t = blockIdx.x, + gridDim.x, ...  Two raw buffers
+// receive whole tiles by cp.async.bulk.tensor (one thread issues, an mbarrier
+// counts the bytes); the copy of tile t + 2*gridDim.x is issued as soon as
+// tile t's raw buffer has been consumed, so the memory system always has the
+// next tile in flight while the current one is transformed.
+//   x / y: the box (P k, N rows) lands as raw[n * P + p]; adjacent k pencils
+//          2g, 2g+1 are one complex value, read directly by the first stage.
+//   z:     the box (N k, P rows) lands as raw[p * N + n] and is copied into
+//          the padded in-place tile.
+// A wait that does not complete within its poll limit sets *err and leaves
+// the tile loop (the host reports the error after the step).
+// ---------------------------------------------------------------------------
+template <typename T>
+struct RawSrc {
+  const T* raw;
+  int P;
+  QHD void pair(int g, int n, T& a, T& b) const {
+    const typename Vec2<T>::type v = *reinterpret_cast<const typename Vec2<T>::type*>(raw + n * P + 2 * g);
+    a = v.x;
+    b = v.y;
+  }
+};
+
+constexpr uint32_t kTmaPollLimit = 1u << 24;
+
+template <int AXIS, int P>
+__device__ __forceinline__ void tile_origin(const Geom& g, int tile, int& c0, int& c1, int& c2) {
+  if (AXIS == 2) {   // P rows (i, j0..j0+P-1); P divides ny
+    const int row = tile * P;
+    c2 = row / g.ny;
+    c1 = row - c2 * g.ny;
+    c0 = 0;
+  } else {
+    const int kt = g.nz / P;
+    const int outer = tile / kt;
+    c0 = (tile - outer * kt) * P;
+    if (AXIS == 1) { c2 = outer; c1 = 0; }
+    else { c1 = outer; c2 = 0; }
+  }
+}
+
+template <typename T, int N, int AXIS, int P>
+__device__ __forceinline__ void tma_issue_tile(const CUtensorMap* map, T* raw, uint64_t* bar, const Geom& g, int tile) {
+  constexpr int SUB = (N + 255) / 256;     // boxes per tile along the transform axis (box dims <= 256)
+  constexpr int BN = N / SUB;
+  int c0, c1, c2;
+  tile_origin<AXIS, P>(g, tile, c0, c1, c2);
+  mbar_expect_tx(bar, uint32_t(P) * N * sizeof(T));
 #pragma unroll
-    for (int c = 0; c < B; ++c) {
-      const int e = tid + (c0 + c) * NT;
-      if ((E % NT == 0 && PER % B == 0) || (c0 + c < PER && e < E)) {
-        int p, n;
-        tile_elem<AXIS, P, N>(e, p, n);
-        buf[p * LD + n] = v[c];
-      }
-    }
+  for (int sb = 0; sb < SUB; ++sb) {
+    if (AXIS == 2) tma_load_3d(raw + sb * BN, map, bar, c0 + sb * BN, c1, c2);          // only N <= 256 reaches here
+    else if (AXIS == 1) tma_load_3d(raw + sb * BN * P, map, bar, c0, c1 + sb * BN, c2);
+    else tma_load_3d(raw + sb * BN * P, map, bar, c0, c1, c2 + sb * BN);
+  }
+}
+
+template <typename T> constexpr int tma_threads() { return sizeof(T) == 8 ? 128 : 256; }
+
+template <typename T, int N, int AXIS, int P, class Store>
+__global__ void __launch_bounds__(tma_threads<T>(), 2)
+    tma_pass_kernel(const __grid_constant__ CUtensorMap map, Geom g, int kind, Tables<T> tb, Store st, int ntiles,
+                    int* err) {
+  constexpr int NT = tma_threads<T>();
+  constexpr int LD = tile_ld(N);
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  T* raw0 = reinterpret_cast<T*>(smem_raw);
+  T* raw1 = raw0 + P * N;
+  T* work = raw1 + P * N;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(work + ((P * LD + 15) / 16) * 16);
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_fence_init();
   }
   __syncthreads();
-  DevExec ex;
-  r2r_tile_inplace<T, N, P / 2, NT>(ex, tid, kind, buf, tb);
-#pragma unroll
-  for (int c = 0; c < PER; ++c) {
-    const int e = tid + c * NT;
-    if (E % NT == 0 || e < E) {
-      int p, n, i, j, k;
-      tile_elem<AXIS, P, N>(e, p, n);
-      tile_coords<AXIS>(g, tile, P, p, n, i, j, k);
-      st(i, j, k, buf[p * LD + n]);
-    }
+  const int t0 = blockIdx.x;
+  if (tid == 0) {
+    if (t0 < ntiles) tma_issue_tile<T, N, AXIS, P>(&map, raw0, &bar[0], g, t0);
+    if (t0 + int(gridDim.x) < ntiles) tma_issue_tile<T, N, AXIS, P>(&map, raw1, &bar[1], g, t0 + gridDim.x);
   }
+  DevExec ex;
+  int it = 0;
+  for (int t = t0; t < ntiles; t += gridDim.x, ++it) {
+    const int b = it & 1;
+    T* raw = b ? raw1 : raw0;
+    const uint32_t parity = (it >> 1) & 1;
+    // every thread polls; the CTA leaves together if any poll gave up
+    const bool arrived = mbar_wait_bounded(&bar[b], parity, kTmaPollLimit);
+    if (!__syncthreads_and(arrived)) {
+      if (tid == 0) atomicExch(err, 1);
+      break;
+    }
+    const int t_next = t + 2 * int(gridDim.x);
+    auto issue_next = [&]() {
+      if (tid == 0 && t_next < ntiles) {
+        fence_proxy_async_smem();
+        tma_issue_tile<T, N, AXIS, P>(&map, raw, &bar[b], g, t_next);
+      }
+    };
+    if constexpr (AXIS != 2) {
+      const int kt = g.nz / P;
+      const int outer = t / kt, k0 = (t - outer * kt) * P;
+      r2r_tile<T, N, P / 2, NT, false>(ex, tid, kind, reinterpret_cast<Cx<T>*>(work), RawSrc<T>{raw, P},
+                                        GlobSnk<T, AXIS, Store>{st, outer, k0}, tb, issue_next);
+    } else {
+      // dense rows -> padded in-place tile (both sides contiguous in n)
+      for (int e = tid; e < P * N; e += NT) {
+        const int p = e / N, n = e - p * N;
+        work[p * LD + n] = raw[e];
+      }
+      __syncthreads();
+      issue_next();
+      r2r_tile_inplace<T, N, P / 2, NT>(ex, tid, kind, work, tb);
+      const int row0 = t * P;
+      for (int e = tid; e < P * N; e += NT) {
+        const int p = e / N, n = e - p * N;
+        const int row = row0 + p;
+        const int i = row / g.ny, j = row - i * g.ny;
+        st(i, j, n, work[p * LD + n]);
+      }
+    }
+    __syncthreads();   // the next tile's first stage overwrites `work`
+  }
+}
+
+template <typename T, int N, int P>
+inline size_t tma_smem_bytes() {
+  return size_t(2) * P * N * sizeof(T) + size_t((P * tile_ld(N) + 15) / 16) * 16 * sizeof(T) + 64;
 }
 
 // Pencils per tile.  z: rows per CTA; x/y: consecutive k (coalescing width).
@@ -139,6 +369,45 @@ cudaError_t launch_pass_n(const Geom& g, int kind, Tables<T> tb, Load ld, Store 
   else if (AXIS == 1) tiles = g.nx * (g.nz / P);
   else tiles = g.ny * (g.nz / P);
   kern<<<tiles, pass_threads<T>(), smem, s>>>(g, kind, tb, ld, st);
+  return cudaGetLastError();
+}
+
+// Plain field loads take the persistent TMA path when the tile fits a box
+// (z: P divides ny and nz <= 256); `tma_err` receives wait timeouts.
+struct TmaConfig {
+  int* err = nullptr;     // device flag, nonzero after a timed-out wait
+  int sms = 148;          // CTAs per SM x SMs bounds the persistent grid
+  bool enabled = true;
+};
+inline TmaConfig& tma_config() {
+  static thread_local TmaConfig c;
+  return c;
+}
+
+template <typename T, int N, int AXIS, int P, class Store>
+cudaError_t launch_tma_pass(const Geom& g, int kind, Tables<T> tb, const T* src, Store st, cudaStream_t s) {
+  uint32_t box[3];
+  constexpr int SUB = (N + 255) / 256;
+  if (AXIS == 2) { box[0] = N; box[1] = P; box[2] = 1; }
+  else if (AXIS == 1) { box[0] = P; box[1] = N / SUB; box[2] = 1; }
+  else { box[0] = P; box[1] = 1; box[2] = N / SUB; }
+  CUtensorMap map;
+  if (!MapCache::get().lookup(&map, src, int(sizeof(T)), g.nx, g.ny, g.nz, AXIS, box)) return cudaErrorNotSupported;
+  const size_t smem = tma_smem_bytes<T, N, P>();
+  auto kern = tma_pass_kernel<T, N, AXIS, P, Store>;
+  static bool configured = false;   // per instantiation
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  int tiles;
+  if (AXIS == 2) tiles = (g.nx * g.ny) / P;
+  else if (AXIS == 1) tiles = g.nx * (g.nz / P);
+  else tiles = g.ny * (g.nz / P);
+  const int per_sm = smem * 2 <= 220 * 1024 ? 2 : 1;
+  const int grid = tiles < per_sm * tma_config().sms ? tiles : per_sm * tma_config().sms;
+  kern<<<grid, tma_threads<T>(), smem, s>>>(map, g, kind, tb, st, tiles, tma_config().err);
   return cudaGetLastError();
 }
 
@@ -170,33 +439,34 @@ cudaError_t launch_pass(const Geom& g, int kind, Tables<T> tb, Load ld, Store st
 #undef QUASI_PASS_CASE
 }
 
-// ---------------------------------------------------------------------------
-// Plain loaders / storers
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ size_t lin(const Geom& g, int i, int j, int k) {
-  return (size_t(i) * g.ny + j) * g.nz + k;
+// Plain field loads: the persistent TMA kernel when the tile fits a box,
+// otherwise the general kernel above.
+template <typename T, int AXIS, class Store>
+cudaError_t launch_pass(const Geom& g, int kind, Tables<T> tb, LoadField<T> ld, Store st, cudaStream_t s) {
+  const int n = AXIS == 0 ? g.nx : (AXIS == 1 ? g.ny : g.nz);
+  const long extent = AXIS == 2 ? long(g.nx) * g.ny : long(g.nz);
+  if (tma_config().enabled && tma_config().err) {
+#define QUASI_TMA_CASE(NN)                                                                             \
+    case NN: {                                                                                         \
+      constexpr int P = pass_pencils<T>(NN);                                                           \
+      const bool fits = extent % P == 0 && (AXIS != 2 || (NN <= 256 && g.ny % P == 0));                \
+      if (fits) return launch_tma_pass<T, NN, AXIS, P>(g, kind, tb, ld.src, st, s);                    \
+      break;                                                                                           \
+    }
+    switch (n) {
+      QUASI_TMA_CASE(16)
+      QUASI_TMA_CASE(32)
+      QUASI_TMA_CASE(64)
+      QUASI_TMA_CASE(96)
+      QUASI_TMA_CASE(128)
+      QUASI_TMA_CASE(192)
+      QUASI_TMA_CASE(256)
+      QUASI_TMA_CASE(512)
+      default: break;
+    }
+#undef QUASI_TMA_CASE
+  }
+  return launch_pass<T, AXIS, LoadField<T>, Store>(g, kind, tb, ld, st, s);
 }
-
-template <typename T>
-struct LoadField {
-  Geom g;
-  const T* src;
-  __device__ T operator()(int i, int j, int k) const { return src[lin(g, i, j, k)]; }
-};
-
-template <typename T>
-struct StoreField {
-  Geom g;
-  T* dst;
-  __device__ void operator()(int i, int j, int k, T v) const { dst[lin(g, i, j, k)] = v; }
-};
-
-template <typename T>
-struct ScaleStore {
-  Geom g;
-  T* dst;
-  T s;
-  __device__ void operator()(int i, int j, int k, T v) const { dst[lin(g, i, j, k)] = v * s; }
-};
 
 }  // namespace quasi

@@ -26,8 +26,11 @@ struct StepCtx {
   int variant, divv_switch, n0;   // n0: planes per emulated MPI rank (quasi.cpp:1641-1690)
   const int* nloop;               // device step counter (the reference's nLoop)
   int store_dtpsi;
-  // spectral state (scaled as the reference scales them)
-  T *psiq, *psiq_old, *Nq, *Nq_old, *rhoq, *divvq, *Sx, *Sy, *Sz;
+  // spectral state (scaled as the reference scales them).  psiq, psiq_old and
+  // psiq_new rotate through three buffers and Nq, Nq_old through two (one
+  // captured graph per phase of the rotation), so the update writes its
+  // result into a buffer nobody reads in that pass.
+  T *psiq, *psiq_old, *psiq_new, *Nq, *Nq_old, *rhoq, *divvq, *Sx, *Sy, *Sz;
   // real fields
   T *psi, *psi_old, *rho, *rho_old, *vx, *vy, *vz, *divv, *p, *df, *lap;
   T *gx, *gy, *gz, *rdx, *rdy, *rdz, *ldx, *ldy, *ldz, *sh, *dtpsi, *tmp;
@@ -94,109 +97,6 @@ template <typename T, int A, bool LAP> struct LdGrad {
   }
 };
 
-// Pressure from the divergence of the shifted stress  quasi.cpp:1379-1414,
-// quasi-stb.cpp:1397-1404 (mask i*j*k > 0 and (4/3)*nu*divv with 4/3 == 1).
-template <typename T> struct LdP {
-  StepCtx<T> c;
-  __device__ T operator()(int i, int j, int k) const {
-    const bool on = c.variant == kQuasi ? (i + j + k != 0) : (i * j * k > 0);
-    if (!on) return T(0);
-    const double sx = i > 0 ? double(c.Sx[at(c, i - 1, j, k)]) : 0.0;
-    const double sy = j > 0 ? double(c.Sy[at(c, i, j - 1, k)]) : 0.0;
-    const double sz = k > 0 ? double(c.Sz[at(c, i, j, k - 1)]) : 0.0;
-    const double q2 = mq2c(c, i, j, k);
-    double v = -(c.vqx[i] * sx + c.vqy[j] * sy + c.vqz[k] * sz) / q2;
-    if (c.variant == kStb) v += c.nu * double(c.divvq[at(c, i, j, k)]);
-    return T(c.scale * v);
-  }
-};
-
-// Staggered Stokes projection of the stress, quasi.cpp:1420-1872.
-template <typename T> struct LdVx {
-  StepCtx<T> c;
-  __device__ T operator()(int i, int j, int k) const {
-    if (i >= c.g.nx - 1) return T(0);   // last global x plane stays 0 (:1522-1548)
-    const double sx = double(c.Sx[at(c, i, j, k)]);
-    const double sy = j > 0 ? double(c.Sy[at(c, i + 1, j - 1, k)]) : 0.0;
-    const double sz = k > 0 ? double(c.Sz[at(c, i + 1, j, k - 1)]) : 0.0;
-    const double vs = c.vsx[i];
-    const double mq = sq(vs) + sq(c.vqy[j]) + sq(c.vqz[k]);
-    const double cm1 = c.scale / (c.nu * mq), cm2 = vs / mq;   // :889-891
-    const double dot = vs * sx + c.vqy[j] * sy + c.vqz[k] * sz;
-    return T(cm1 * (sx - cm2 * dot + c.nu * vs * double(c.divvq[at(c, i + 1, j, k)])));
-  }
-};
-
-// Sx at the plane "i-1" as halo #4 delivers it: on emulated rank r >= 1 the
-// rank's first plane receives the previous rank's FIRST plane (quasi.cpp:1649).
-template <typename T>
-__device__ __forceinline__ int halo4_src(const StepCtx<T>& c, int i) {
-  return (i % c.n0 == 0) ? i - c.n0 : i - 1;
-}
-
-template <typename T> struct LdVy {
-  StepCtx<T> c;
-  __device__ T operator()(int i, int j, int k) const {
-    if (j >= c.g.ny - 1 || k >= c.g.nz - 1) return T(0);   // :1684-1685,1728-1730
-    const double sx = i > 0 ? double(c.Sx[at(c, halo4_src(c, i), j + 1, k)]) : 0.0;
-    const double sy = double(c.Sy[at(c, i, j, k)]);
-    const double sz = k > 0 ? double(c.Sz[at(c, i, j + 1, k - 1)]) : 0.0;
-    const double vs = c.vsy[j];
-    const double mq = sq(c.vqx[i]) + sq(vs) + sq(c.vqz[k]);
-    const double cm1 = c.scale / (c.nu * mq), cm2 = vs / mq;   // :893-895
-    const double dot = c.vqx[i] * sx + vs * sy + c.vqz[k] * sz;
-    return T(cm1 * (sy - cm2 * dot + c.nu * vs * double(c.divvq[at(c, i, j + 1, k)])));
-  }
-};
-
-template <typename T> struct LdVz {
-  StepCtx<T> c;
-  __device__ T operator()(int i, int j, int k) const {
-    if (j >= c.g.ny - 1 || k >= c.g.nz - 1) return T(0);
-    const double sx = i > 0 ? double(c.Sx[at(c, halo4_src(c, i), j, k + 1)]) : 0.0;
-    const double sy = j > 0 ? double(c.Sy[at(c, i, j - 1, k + 1)]) : 0.0;
-    const double sz = double(c.Sz[at(c, i, j, k)]);
-    const double vs = c.vsz[k];
-    const double mq = sq(c.vqx[i]) + sq(c.vqy[j]) + sq(vs);
-    const double cm1 = c.scale / (c.nu * mq), cm2 = vs / mq;   // :897-899
-    const double dot = c.vqx[i] * sx + c.vqy[j] * sy + vs * sz;
-    return T(cm1 * (sz - cm2 * dot + c.nu * vs * double(c.divvq[at(c, i, j, k + 1)])));
-  }
-};
-
-// divv = iCT(scale divvq)                                    quasi.cpp:1888-1900
-template <typename T> struct LdDivvOut {
-  StepCtx<T> c;
-  __device__ T operator()(int i, int j, int k) const { return T(c.scale * double(c.divvq[at(c, i, j, k)])); }
-};
-
-// Semi-implicit update (quasi.cpp:1944-1962, quasi-stb.cpp:1946-1958), with the
-// state shuffles psiq_old <- psiq, psiq <- new, Nq_old <- Nq folded in.
-template <typename T> struct LdUpdate {
-  StepCtx<T> c;
-  __device__ T operator()(int i, int j, int k) const {
-    const size_t id = at(c, i, j, k);
-    const double q2 = mq2c(c, i, j, k);
-    const double alin = c.ep - c.alpha * sq(c.q0 * c.q0 - q2);
-    const double pq = double(c.psiq[id]);
-    const double nq = double(c.Nq[id]);
-    const double nq_old = (*c.nloop == 1) ? nq : double(c.Nq_old[id]);   // :1936-1938
-    const double dtd2 = c.dt / 2;
-    double nv;
-    if (c.variant == kQuasi) {
-      const double c1 = 2.0 - c.dt * c.rho_m * alin, c2 = 1.5 - c.dt * c.rho_m * alin;   // :886-887
-      nv = (c1 * pq - 0.5 * double(c.psiq_old[id]) + dtd2 * c.scale * (3.0 * nq - nq_old)) / c2;
-    } else {
-      const double c1 = 1.0 + dtd2 * alin, c2 = 1.0 - dtd2 * alin;   // quasi-stb.cpp:855-856
-      nv = (c1 * pq + dtd2 * c.scale * (3.0 * nq - nq_old)) / c2;
-    }
-    c.psiq_old[id] = T(pq);
-    c.psiq[id] = T(nv);
-    c.Nq_old[id] = T(nq);
-    return T(nv);
-  }
-};
-
 // ---------------------------------------------------------------------------
 // Real-space loaders (first, z-axis pass of forward transforms)
 // ---------------------------------------------------------------------------
@@ -208,50 +108,6 @@ template <typename T> struct LdRhoRaw {
     const size_t id = at(c, i, j, k);
     const double ps = c.psi[id], x = c.gx[id], y = c.gy[id], z = c.gz[id];
     return T(c.kp * sqrt(c.q0 * c.q0 * ps * ps + x * x + y * y + z * z) + c.rho0);
-  }
-};
-
-// Stress S_a (quasi.cpp:1305-1317) / mu grad psi (quasi-stb.cpp:1295-1305)
-template <typename T, int A> struct LdS {
-  StepCtx<T> c;
-  __device__ T operator()(int i, int j, int k) const {
-    const size_t id = at(c, i, j, k);
-    const double g = A == 0 ? c.gx[id] : (A == 1 ? c.gy[id] : c.gz[id]);
-    if (c.variant == kQuasi) {
-      const double rho = c.rho[id];
-      const double lr = rho * double(c.lap[id]);
-      const double ld = A == 0 ? c.ldx[id] : (A == 1 ? c.ldy[id] : c.ldz[id]);
-      return T(lr * g - rho * double(c.df[id]) * ld);
-    }
-    const double ps = c.psi[id];
-    const double mu = double(c.sh[id]) - c.beta * ps * ps * ps + c.gamma * ps * ps * ps * ps * ps;
-    return T(mu * g);   // rho == 1
-  }
-};
-
-// Nonlinear term N (quasi.cpp:1905-1929, quasi-stb.cpp:1900-1924)
-template <typename T> struct LdN {
-  StepCtx<T> c;
-  __device__ T operator()(int i, int j, int k) const {
-    const size_t id = at(c, i, j, k);
-    const double ps = c.psi[id];
-    const double p3 = ps * ps * ps, p5 = p3 * ps * ps;
-    const double adv = double(c.vx[id]) * double(c.gx[id]) + double(c.vy[id]) * double(c.gy[id]) +
-                       double(c.vz[id]) * double(c.gz[id]);
-    if (c.variant == kQuasi) {
-      const double rho = c.rho[id];
-      double n = rho * (c.ep * ps - double(c.df[id]) + c.beta * p3 - c.gamma * p5) - rho * double(c.lap[id]) - adv;
-      if (*c.nloop > c.divv_switch + 1) {
-        const double a = c.rdx[id], b = c.rdy[id], d = c.rdz[id];
-        n += double(c.p[id]) * c.kp * sqrt(a * a + b * b + d * d) / (c.rho_s * c.rho_s);
-      }
-      return T(n);
-    }
-    if (c.store_dtpsi) {
-      const double mu = double(c.sh[id]) - c.beta * p3 + c.gamma * p5;
-      c.dtpsi[id] = T(-mu - adv);   // quasi-stb.cpp:1909-1912, rho == 1
-    }
-    return T(c.beta * p3 - c.gamma * p5 - adv);
   }
 };
 
@@ -274,23 +130,6 @@ template <typename T> struct StRhoq {
   }
 };
 
-// smoothed rho, divv (after the switch) and rho_old          quasi.cpp:1267-1285
-template <typename T> struct StRho {
-  StepCtx<T> c;
-  __device__ void operator()(int i, int j, int k, T v) const {
-    const size_t id = at(c, i, j, k);
-    const double r = v;
-    if (*c.nloop > c.divv_switch) {
-      const double ro = c.rho_old[id];
-      const double adv = double(c.vx[id]) * double(c.rdx[id]) + double(c.vy[id]) * double(c.rdy[id]) +
-                         double(c.vz[id]) * double(c.rdz[id]);
-      c.divv[id] = T(-((r - ro) / c.dt + adv) / (0.5 * (r + ro)));
-    }
-    c.rho[id] = v;
-    c.rho_old[id] = v;
-  }
-};
-
 // psi_old <- psi, psi <- iCT(psiq')                           quasi.cpp:1961-1965
 template <typename T> struct StPsi {
   StepCtx<T> c;
@@ -300,6 +139,181 @@ template <typename T> struct StPsi {
     c.psi[id] = v;
   }
 };
+
+// ---------------------------------------------------------------------------
+// Elementwise stages.  Each reads every input field once, fully coalesced
+// (consecutive threads -> consecutive k), computes the terms shared by its
+// outputs once, and leaves the transforms around it plain.
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ void unlin(const Geom& g, size_t id, int& i, int& j, int& k) {
+  k = int(id % g.nz);
+  const size_t r = id / g.nz;
+  j = int(r % g.ny);
+  i = int(r / g.ny);
+}
+
+// divv (after the switch) and rho_old <- rho          quasi.cpp:1273-1289
+template <typename T>
+__global__ void __launch_bounds__(256) divv_kernel(StepCtx<T> c, size_t n) {
+  const bool on = *c.nloop > c.divv_switch;
+  for (size_t id = blockIdx.x * size_t(blockDim.x) + threadIdx.x; id < n; id += size_t(gridDim.x) * blockDim.x) {
+    const double r = c.rho[id];
+    if (on) {
+      const double ro = c.rho_old[id];
+      const double adv = double(c.vx[id]) * double(c.rdx[id]) + double(c.vy[id]) * double(c.rdy[id]) +
+                         double(c.vz[id]) * double(c.rdz[id]);
+      c.divv[id] = T(-((r - ro) / c.dt + adv) / (0.5 * (r + ro)));
+    }
+    c.rho_old[id] = T(r);
+  }
+}
+
+// stress S (quasi.cpp:1305-1317) or mu grad psi (quasi-stb.cpp:1295-1305)
+template <typename T>
+__global__ void __launch_bounds__(256) stress_kernel(StepCtx<T> c, size_t n) {
+  for (size_t id = blockIdx.x * size_t(blockDim.x) + threadIdx.x; id < n; id += size_t(gridDim.x) * blockDim.x) {
+    const double gx = c.gx[id], gy = c.gy[id], gz = c.gz[id];
+    if (c.variant == kQuasi) {
+      const double rho = c.rho[id];
+      const double lr = rho * double(c.lap[id]);
+      const double rd = rho * double(c.df[id]);
+      c.Sx[id] = T(lr * gx - rd * double(c.ldx[id]));
+      c.Sy[id] = T(lr * gy - rd * double(c.ldy[id]));
+      c.Sz[id] = T(lr * gz - rd * double(c.ldz[id]));
+    } else {
+      const double ps = c.psi[id];
+      const double mu = double(c.sh[id]) - c.beta * ps * ps * ps + c.gamma * ps * ps * ps * ps * ps;
+      c.Sx[id] = T(mu * gx);
+      c.Sy[id] = T(mu * gy);
+      c.Sz[id] = T(mu * gz);
+    }
+  }
+}
+
+// Pressure, staggered Stokes projection and scaled divv, from the spectral
+// stress: quasi.cpp:1379-1414 (p), 1420-1872 (v), 1888-1894 (divv).  Writes
+// p^ -> p, v^ -> vx/vy/vz, scale*divv^ -> divv; the inverse transforms that
+// follow run in place on those fields.
+template <typename T>
+__global__ void __launch_bounds__(256) project_kernel(StepCtx<T> c, size_t n) {
+  const Geom g = c.g;
+  for (size_t id = blockIdx.x * size_t(blockDim.x) + threadIdx.x; id < n; id += size_t(gridDim.x) * blockDim.x) {
+    int i, j, k;
+    unlin<T>(g, id, i, j, k);
+    const size_t sj = g.nz, si = size_t(g.ny) * g.nz;
+    const double qx = c.vqx[i], qy = c.vqy[j], qz = c.vqz[k];
+    const double sxc = c.Sx[id], syc = c.Sy[id], szc = c.Sz[id];
+    const double dvc = c.divvq[id];
+    // p^: divergence of the stress shifted back onto the cosine grid
+    {
+      const bool on = c.variant == kQuasi ? (i + j + k != 0) : (i * j * k > 0);
+      double pv = 0.0;
+      if (on) {
+        const double sx = i > 0 ? double(c.Sx[id - si]) : 0.0;
+        const double sy = j > 0 ? double(c.Sy[id - sj]) : 0.0;
+        const double sz = k > 0 ? double(c.Sz[id - 1]) : 0.0;
+        const double q2 = qx * qx + qy * qy + qz * qz;
+        double v = -(qx * sx + qy * sy + qz * sz) / q2;
+        if (c.variant == kStb) v += c.nu * dvc;
+        pv = c.scale * v;
+      }
+      c.p[id] = T(pv);
+    }
+    // v^x (i < nx-1)
+    {
+      double v = 0.0;
+      if (i < g.nx - 1) {
+        const double sy = j > 0 ? double(c.Sy[id + si - sj]) : 0.0;
+        const double sz = k > 0 ? double(c.Sz[id + si - 1]) : 0.0;
+        const double vs = c.vsx[i];
+        const double mq = vs * vs + qy * qy + qz * qz;
+        const double dot = vs * sxc + qy * sy + qz * sz;
+        v = (c.scale / (c.nu * mq)) * (sxc - (vs / mq) * dot + c.nu * vs * double(c.divvq[id + si]));
+      }
+      c.vx[id] = T(v);
+    }
+    // v^y, v^z (j < ny-1, k < nz-1); Sx from the plane halo #4 delivers (quasi.cpp:1649)
+    double vy = 0.0, vz = 0.0;
+    if (j < g.ny - 1 && k < g.nz - 1) {
+      const int isrc = (i % c.n0 == 0) ? i - c.n0 : i - 1;
+      const size_t bx = size_t(isrc) * si + size_t(j) * sj + k;
+      {
+        const double sx = i > 0 ? double(c.Sx[bx + sj]) : 0.0;
+        const double sz = k > 0 ? double(c.Sz[id + sj - 1]) : 0.0;
+        const double vs = c.vsy[j];
+        const double mq = qx * qx + vs * vs + qz * qz;
+        const double dot = qx * sx + vs * syc + qz * sz;
+        vy = (c.scale / (c.nu * mq)) * (syc - (vs / mq) * dot + c.nu * vs * double(c.divvq[id + sj]));
+      }
+      {
+        const double sx = i > 0 ? double(c.Sx[bx + 1]) : 0.0;
+        const double sy = j > 0 ? double(c.Sy[id - sj + 1]) : 0.0;
+        const double vs = c.vsz[k];
+        const double mq = qx * qx + qy * qy + vs * vs;
+        const double dot = qx * sx + qy * sy + vs * szc;
+        vz = (c.scale / (c.nu * mq)) * (szc - (vs / mq) * dot + c.nu * vs * double(c.divvq[id + 1]));
+      }
+    }
+    c.vy[id] = T(vy);
+    c.vz[id] = T(vz);
+    if (c.variant == kQuasi) c.divv[id] = T(c.scale * dvc);
+  }
+}
+
+// Nonlinear term N (quasi.cpp:1905-1929, quasi-stb.cpp:1900-1924) -> Nq
+template <typename T>
+__global__ void __launch_bounds__(256) nonlinear_kernel(StepCtx<T> c, size_t n) {
+  const bool pcoup = *c.nloop > c.divv_switch + 1;
+  for (size_t id = blockIdx.x * size_t(blockDim.x) + threadIdx.x; id < n; id += size_t(gridDim.x) * blockDim.x) {
+    const double ps = c.psi[id];
+    const double p3 = ps * ps * ps, p5 = p3 * ps * ps;
+    const double adv = double(c.vx[id]) * double(c.gx[id]) + double(c.vy[id]) * double(c.gy[id]) +
+                       double(c.vz[id]) * double(c.gz[id]);
+    double nv;
+    if (c.variant == kQuasi) {
+      const double rho = c.rho[id];
+      nv = rho * (c.ep * ps - double(c.df[id]) + c.beta * p3 - c.gamma * p5) - rho * double(c.lap[id]) - adv;
+      if (pcoup) {
+        const double a = c.rdx[id], b = c.rdy[id], d = c.rdz[id];
+        nv += double(c.p[id]) * c.kp * sqrt(a * a + b * b + d * d) / (c.rho_s * c.rho_s);
+      }
+    } else {
+      if (c.store_dtpsi) {
+        const double mu = double(c.sh[id]) - c.beta * p3 + c.gamma * p5;
+        c.dtpsi[id] = T(-mu - adv);   // quasi-stb.cpp:1909-1912, rho == 1
+      }
+      nv = c.beta * p3 - c.gamma * p5 - adv;
+    }
+    c.Nq[id] = T(nv);
+  }
+}
+
+// Semi-implicit update -> psiq_new (quasi.cpp:1944-1962, quasi-stb.cpp:1946-1958)
+template <typename T>
+__global__ void __launch_bounds__(256) update_kernel(StepCtx<T> c, size_t n) {
+  const Geom g = c.g;
+  const bool first = *c.nloop == 1;
+  for (size_t id = blockIdx.x * size_t(blockDim.x) + threadIdx.x; id < n; id += size_t(gridDim.x) * blockDim.x) {
+    int i, j, k;
+    unlin<T>(g, id, i, j, k);
+    const double q2 = mq2c(c, i, j, k);
+    const double alin = c.ep - c.alpha * sq(c.q0 * c.q0 - q2);
+    const double pq = c.psiq[id];
+    const double nq = c.Nq[id];
+    const double nq_old = first ? nq : double(c.Nq_old[id]);   // :1936-1938
+    const double dtd2 = c.dt / 2;
+    double nv;
+    if (c.variant == kQuasi) {
+      const double c1 = 2.0 - c.dt * c.rho_m * alin, c2 = 1.5 - c.dt * c.rho_m * alin;   // :886-887
+      nv = (c1 * pq - 0.5 * double(c.psiq_old[id]) + dtd2 * c.scale * (3.0 * nq - nq_old)) / c2;
+    } else {
+      const double c1 = 1.0 + dtd2 * alin, c2 = 1.0 - dtd2 * alin;   // quasi-stb.cpp:855-856
+      nv = (c1 * pq + dtd2 * c.scale * (3.0 * nq - nq_old)) / c2;
+    }
+    c.psiq_new[id] = T(nv);
+  }
+}
 
 // ---------------------------------------------------------------------------
 // 3-D transforms as three passes
@@ -349,13 +363,17 @@ static __global__ void bump_counter_kernel(int* n) { *n += 1; }
     if (e_ != cudaSuccess) return e_;         \
   } while (0)
 
+constexpr int kEwBlocks = 148 * 8;   // elementwise grid: 8 x 256 threads per SM
+
 // One time step, enqueued on `s` (captured into a CUDA graph by the caller).
 template <typename T>
 cudaError_t enqueue_step(const StepCtx<T>& c, const AxisTables<T>& tb, int* nloop_dev, cudaStream_t s) {
   const Geom g = c.g;
+  const size_t n = size_t(g.nx) * g.ny * g.nz;
   bump_counter_kernel<<<1, 1, 0, s>>>(nloop_dev);
   QUASI_TRY(cudaGetLastError());
   auto st = [&](T* d) { return StoreField<T>{g, d}; };
+  auto ld = [&](T* d) { return LoadField<T>{g, d}; };
   if (c.variant == kQuasi) {
     // a3 prologue quasi.cpp:1036-1057
     QUASI_TRY(inverse3(g, tb, kiCT, LdDf<T>{c}, c.df, st(c.df), s));
@@ -372,15 +390,11 @@ cudaError_t enqueue_step(const StepCtx<T>& c, const AxisTables<T>& tb, int* nloo
     QUASI_TRY(inverse3(g, tb, kiSTz, LdGrad<T, 2, true>{c, c.psiq}, c.ldz, st(c.ldz), s));
     // a5 density + filter quasi.cpp:1237-1268 (rho doubles as the scratch)
     QUASI_TRY(forward3(g, tb, kCT, LdRhoRaw<T>{c}, c.rho, StRhoq<T>{c}, s));
-    QUASI_TRY(inverse3(g, tb, kiCT, LdRealField<T>{c, c.rhoq}, c.rho, StRho<T>{c}, s));
-    // a6 divv -> spectral quasi.cpp:1290-1293
-    QUASI_TRY(forward3(g, tb, kCT, LdRealField<T>{c, c.divv}, c.divvq, st(c.divvq), s));
-    // a7 stress quasi.cpp:1298-1330
-    QUASI_TRY(forward3(g, tb, kSTx, LdS<T, 0>{c}, c.Sx, st(c.Sx), s));
-    QUASI_TRY(forward3(g, tb, kSTy, LdS<T, 1>{c}, c.Sy, st(c.Sy), s));
-    QUASI_TRY(forward3(g, tb, kSTz, LdS<T, 2>{c}, c.Sz, st(c.Sz), s));
-    // a8 pressure quasi.cpp:1379-1418
-    QUASI_TRY(inverse3(g, tb, kiCT, LdP<T>{c}, c.p, st(c.p), s));
+    QUASI_TRY(inverse3(g, tb, kiCT, ld(c.rhoq), c.rho, st(c.rho), s));
+    // a6 divv quasi.cpp:1273-1293
+    divv_kernel<T><<<kEwBlocks, 256, 0, s>>>(c, n);
+    QUASI_TRY(cudaGetLastError());
+    QUASI_TRY(forward3(g, tb, kCT, ld(c.divv), c.divvq, st(c.divvq), s));
   } else {
     // quasi-stb.cpp:1005-1038 (the unused dRho transform is elided)
     QUASI_TRY(inverse3(g, tb, kiCT, LdSh<T>{c}, c.sh, st(c.sh), s));
@@ -388,22 +402,29 @@ cudaError_t enqueue_step(const StepCtx<T>& c, const AxisTables<T>& tb, int* nloo
     QUASI_TRY(inverse3(g, tb, kiSTy, LdGrad<T, 1, false>{c, c.psiq}, c.gy, st(c.gy), s));
     QUASI_TRY(inverse3(g, tb, kiSTz, LdGrad<T, 2, false>{c, c.psiq}, c.gz, st(c.gz), s));
     // rho == 1, divv == 0, grad rho == 0 (rhoq never leaves 0): quasi-stb.cpp:1232
-    QUASI_TRY(forward3(g, tb, kSTx, LdS<T, 0>{c}, c.Sx, st(c.Sx), s));
-    QUASI_TRY(forward3(g, tb, kSTy, LdS<T, 1>{c}, c.Sy, st(c.Sy), s));
-    QUASI_TRY(forward3(g, tb, kSTz, LdS<T, 2>{c}, c.Sz, st(c.Sz), s));
   }
-  // a9 velocity quasi.cpp:1420-1884
-  QUASI_TRY(inverse3(g, tb, kiSTx, LdVx<T>{c}, c.vx, st(c.vx), s));
-  QUASI_TRY(inverse3(g, tb, kiSTy, LdVy<T>{c}, c.vy, st(c.vy), s));
-  QUASI_TRY(inverse3(g, tb, kiSTz, LdVz<T>{c}, c.vz, st(c.vz), s));
-  if (c.variant == kQuasi) {
-    // a10 divv out quasi.cpp:1888-1900
-    QUASI_TRY(inverse3(g, tb, kiCT, LdDivvOut<T>{c}, c.divv, st(c.divv), s));
-  }
+  // a7 stress quasi.cpp:1298-1330
+  stress_kernel<T><<<kEwBlocks, 256, 0, s>>>(c, n);
+  QUASI_TRY(cudaGetLastError());
+  QUASI_TRY(forward3(g, tb, kSTx, ld(c.Sx), c.Sx, st(c.Sx), s));
+  QUASI_TRY(forward3(g, tb, kSTy, ld(c.Sy), c.Sy, st(c.Sy), s));
+  QUASI_TRY(forward3(g, tb, kSTz, ld(c.Sz), c.Sz, st(c.Sz), s));
+  // a8 pressure, a9 velocity, a10 scaled divv quasi.cpp:1336-1900
+  project_kernel<T><<<kEwBlocks, 256, 0, s>>>(c, n);
+  QUASI_TRY(cudaGetLastError());
+  if (c.variant == kQuasi) QUASI_TRY(inverse3(g, tb, kiCT, ld(c.p), c.p, st(c.p), s));
+  QUASI_TRY(inverse3(g, tb, kiSTx, ld(c.vx), c.vx, st(c.vx), s));
+  QUASI_TRY(inverse3(g, tb, kiSTy, ld(c.vy), c.vy, st(c.vy), s));
+  QUASI_TRY(inverse3(g, tb, kiSTz, ld(c.vz), c.vz, st(c.vz), s));
+  if (c.variant == kQuasi) QUASI_TRY(inverse3(g, tb, kiCT, ld(c.divv), c.divv, st(c.divv), s));
   // a11 nonlinear term quasi.cpp:1905-1939
-  QUASI_TRY(forward3(g, tb, kCT, LdN<T>{c}, c.Nq, st(c.Nq), s));
+  nonlinear_kernel<T><<<kEwBlocks, 256, 0, s>>>(c, n);
+  QUASI_TRY(cudaGetLastError());
+  QUASI_TRY(forward3(g, tb, kCT, ld(c.Nq), c.Nq, st(c.Nq), s));
   // a12 update + iCT quasi.cpp:1944-1965
-  QUASI_TRY(inverse3(g, tb, kiCT, LdUpdate<T>{c}, c.tmp, StPsi<T>{c}, s));
+  update_kernel<T><<<kEwBlocks, 256, 0, s>>>(c, n);
+  QUASI_TRY(cudaGetLastError());
+  QUASI_TRY(inverse3(g, tb, kiCT, ld(c.psiq_new), c.tmp, StPsi<T>{c}, s));
   return cudaSuccess;
 }
 
@@ -422,7 +443,7 @@ template <typename T> struct LdInitN {
 template <typename T>
 __global__ void init_state_kernel(StepCtx<T> c, size_t n) {
   for (size_t id = blockIdx.x * size_t(blockDim.x) + threadIdx.x; id < n; id += size_t(gridDim.x) * blockDim.x) {
-    c.psiq_old[id] = c.psiq[id];
+    c.psiq_old[id] = c.psiq[id];   // quasi.cpp:939
     c.psi_old[id] = c.psi[id];
     c.divv[id] = T(0);
     c.divvq[id] = T(0);
@@ -441,7 +462,7 @@ cudaError_t enqueue_init(const StepCtx<T>& c, const AxisTables<T>& tb, int* nloo
   const Geom g = c.g;
   QUASI_TRY(forward3(g, tb, kCT, LdRealField<T>{c, c.psi}, c.psiq, ScaleStore<T>{g, c.psiq, T(c.scale)}, s));
   QUASI_TRY(inverse3(g, tb, kiCT, LdRealField<T>{c, c.psiq}, c.psi, StoreField<T>{g, c.psi}, s));
-  QUASI_TRY(forward3(g, tb, kCT, LdInitN<T>{c}, c.Nq, StoreField<T>{g, c.Nq}, s));
+  QUASI_TRY(forward3(g, tb, kCT, LdInitN<T>{c}, c.Nq_old, StoreField<T>{g, c.Nq_old}, s));
   const size_t n = size_t(g.nx) * g.ny * g.nz;
   init_state_kernel<T><<<592, 256, 0, s>>>(c, n);
   QUASI_TRY(cudaGetLastError());
