@@ -125,6 +125,7 @@ class Engine : public EngineBase {
   }
 
   int set_psi(const double* host) override {
+    set_phase(0);   // quasi_init starts the rotation at phase 0
     T* st = static_cast<T*>(host_stage_);
     for (size_t i = 0; i < n_; ++i) st[i] = T(host[i]);
     if (!cuda_ok(cudaMemcpyAsync(c_.psi, st, n_ * sizeof(T), cudaMemcpyHostToDevice, stream_), "H2D")) return QUASI_ERR_CUDA;
@@ -184,6 +185,7 @@ class Engine : public EngineBase {
   int diagnostics(double out[3]) override {
     if (!initialized_) { err = "diagnostics before quasi_init"; return QUASI_ERR_STATE; }
     const int energy = cfg_.variant == QUASI_VARIANT_QUASI;
+    set_phase(nloop_);
     diag_partial_kernel<T><<<kDiagBlocks, kDiagThreads, 0, stream_>>>(c_.psi, c_.psi_old, c_.rho, c_.df, c_.ep, c_.alpha,
                                                                       c_.beta, c_.gamma, energy, n_, partial_);
     diag_final_kernel<<<1, 32, 0, stream_>>>(partial_, kDiagBlocks, partial_ + kDiagBlocks * 4);
@@ -307,13 +309,18 @@ class Engine : public EngineBase {
 
   // Buffer rotation for a step that starts after `s` completed steps:
   // psiq = A[s%3], psiq_old = A[(s+2)%3], psiq_new = A[(s+1)%3];
-  // Nq (computed this step) = B[s%2], Nq_old = B[(s+1)%2].
+  // Nq (computed this step) = B[s%2], Nq_old = B[(s+1)%2];
+  // psi = C[s%2], psi_old = psi_new = C[(s+1)%2] (psi_old is read only by the
+  // diagnostics after the step, when it is C[s%2] again).
   void set_phase(long s) {
     c_.psiq = psiq_buf_[s % 3];
     c_.psiq_old = psiq_buf_[(s + 2) % 3];
     c_.psiq_new = psiq_buf_[(s + 1) % 3];
     c_.Nq = nq_buf_[s % 2];
     c_.Nq_old = nq_buf_[(s + 1) % 2];
+    c_.psi = psi_buf_[s % 2];
+    c_.psi_old = psi_buf_[(s + 1) % 2];
+    c_.psi_new = psi_buf_[(s + 1) % 2];
   }
 
   void use_tma() {
@@ -353,10 +360,11 @@ class Engine : public EngineBase {
     c_.store_dtpsi = quasi ? 0 : 1;
     for (auto& b : psiq_buf_) b = next();
     for (auto& b : nq_buf_) b = next();
+    for (auto& b : psi_buf_) b = next();
     set_phase(0);
     c_.rhoq = next();
     c_.divvq = next(); c_.Sx = next(); c_.Sy = next(); c_.Sz = next();
-    c_.psi = next(); c_.psi_old = next(); c_.rho = next(); c_.rho_old = next();
+    c_.rho = next(); c_.rho_old = next();
     c_.vx = next(); c_.vy = next(); c_.vz = next(); c_.divv = next(); c_.p = next();
     c_.df = next(); c_.lap = next(); c_.gx = next(); c_.gy = next(); c_.gz = next();
     c_.rdx = next(); c_.rdy = next(); c_.rdz = next(); c_.ldx = next(); c_.ldy = next(); c_.ldz = next();
@@ -435,6 +443,7 @@ class Engine : public EngineBase {
   cudaGraphExec_t graph_exec_[kPhases] = {};
   T* psiq_buf_[3] = {};
   T* nq_buf_[2] = {};
+  T* psi_buf_[2] = {};
   int graph_kernels_ = 0;
   long nloop_ = 0;
 };

@@ -236,6 +236,32 @@ struct RawSrc {
   }
 };
 
+// Identity multiplier (plain passes).
+struct NoMul {
+  static constexpr bool kActive = false;
+  __device__ double operator()(int, int, int) const { return 1.0; }
+};
+
+// x / y tile source with a per-element multiplier of the OUTPUT index
+// (i, j, k): the spectral prologue of an inverse transform.
+template <typename T, int AXIS, class Mul>
+struct MulSrc {
+  const T* raw;
+  int P, outer, k0;
+  Mul mul;
+  QHD void pair(int g, int n, T& a, T& b) const {
+    const typename Vec2<T>::type v = *reinterpret_cast<const typename Vec2<T>::type*>(raw + n * P + 2 * g);
+    a = v.x;
+    b = v.y;
+    if constexpr (Mul::kActive) {
+      const int k = k0 + 2 * g;
+      const int i = AXIS == 1 ? outer : n, j = AXIS == 1 ? n : outer;
+      a = T(double(a) * mul(i, j, k));
+      b = T(double(b) * mul(i, j, k + 1));
+    }
+  }
+};
+
 constexpr uint32_t kTmaPollLimit = 1u << 24;
 
 template <int AXIS, int P>
@@ -255,11 +281,14 @@ __device__ __forceinline__ void tile_origin(const Geom& g, int tile, int& c0, in
 }
 
 template <typename T, int N, int AXIS, int P>
-__device__ __forceinline__ void tma_issue_tile(const CUtensorMap* map, T* raw, uint64_t* bar, const Geom& g, int tile) {
+__device__ __forceinline__ void tma_issue_tile(const CUtensorMap* map, T* raw, uint64_t* bar, const Geom& g, int tile,
+                                               int dc1, int dc2) {
   constexpr int SUB = (N + 255) / 256;     // boxes per tile along the transform axis (box dims <= 256)
   constexpr int BN = N / SUB;
   int c0, c1, c2;
   tile_origin<AXIS, P>(g, tile, c0, c1, c2);
+  c1 += dc1;   // shifted loads (j + 1, i + 1): out-of-range rows read as zero
+  c2 += dc2;
   mbar_expect_tx(bar, uint32_t(P) * N * sizeof(T));
 #pragma unroll
   for (int sb = 0; sb < SUB; ++sb) {
@@ -271,10 +300,10 @@ __device__ __forceinline__ void tma_issue_tile(const CUtensorMap* map, T* raw, u
 
 template <typename T> constexpr int tma_threads() { return sizeof(T) == 8 ? 128 : 256; }
 
-template <typename T, int N, int AXIS, int P, class Store>
+template <typename T, int N, int AXIS, int P, class Store, class Mul>
 __global__ void __launch_bounds__(tma_threads<T>(), 2)
     tma_pass_kernel(const __grid_constant__ CUtensorMap map, Geom g, int kind, Tables<T> tb, Store st, int ntiles,
-                    int* err) {
+                    int* err, Mul mul, int dc1, int dc2) {
   constexpr int NT = tma_threads<T>();
   constexpr int LD = tile_ld(N);
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -291,8 +320,9 @@ __global__ void __launch_bounds__(tma_threads<T>(), 2)
   __syncthreads();
   const int t0 = blockIdx.x;
   if (tid == 0) {
-    if (t0 < ntiles) tma_issue_tile<T, N, AXIS, P>(&map, raw0, &bar[0], g, t0);
-    if (t0 + int(gridDim.x) < ntiles) tma_issue_tile<T, N, AXIS, P>(&map, raw1, &bar[1], g, t0 + gridDim.x);
+    if (t0 < ntiles) tma_issue_tile<T, N, AXIS, P>(&map, raw0, &bar[0], g, t0, dc1, dc2);
+    if (t0 + int(gridDim.x) < ntiles)
+      tma_issue_tile<T, N, AXIS, P>(&map, raw1, &bar[1], g, t0 + gridDim.x, dc1, dc2);
   }
   DevExec ex;
   int it = 0;
@@ -310,13 +340,14 @@ __global__ void __launch_bounds__(tma_threads<T>(), 2)
     auto issue_next = [&]() {
       if (tid == 0 && t_next < ntiles) {
         fence_proxy_async_smem();
-        tma_issue_tile<T, N, AXIS, P>(&map, raw, &bar[b], g, t_next);
+        tma_issue_tile<T, N, AXIS, P>(&map, raw, &bar[b], g, t_next, dc1, dc2);
       }
     };
     if constexpr (AXIS != 2) {
       const int kt = g.nz / P;
       const int outer = t / kt, k0 = (t - outer * kt) * P;
-      r2r_tile<T, N, P / 2, NT, false>(ex, tid, kind, reinterpret_cast<Cx<T>*>(work), RawSrc<T>{raw, P},
+      r2r_tile<T, N, P / 2, NT, false>(ex, tid, kind, reinterpret_cast<Cx<T>*>(work),
+                                        MulSrc<T, AXIS, Mul>{raw, P, outer, k0, mul},
                                         GlobSnk<T, AXIS, Store>{st, outer, k0}, tb, issue_next);
     } else {
       // dense rows -> padded in-place tile (both sides contiguous in n)
@@ -384,8 +415,9 @@ inline TmaConfig& tma_config() {
   return c;
 }
 
-template <typename T, int N, int AXIS, int P, class Store>
-cudaError_t launch_tma_pass(const Geom& g, int kind, Tables<T> tb, const T* src, Store st, cudaStream_t s) {
+template <typename T, int N, int AXIS, int P, class Store, class Mul = NoMul>
+cudaError_t launch_tma_pass(const Geom& g, int kind, Tables<T> tb, const T* src, Store st, cudaStream_t s,
+                            Mul mul = Mul(), int dc1 = 0, int dc2 = 0) {
   uint32_t box[3];
   constexpr int SUB = (N + 255) / 256;
   if (AXIS == 2) { box[0] = N; box[1] = P; box[2] = 1; }
@@ -394,7 +426,7 @@ cudaError_t launch_tma_pass(const Geom& g, int kind, Tables<T> tb, const T* src,
   CUtensorMap map;
   if (!MapCache::get().lookup(&map, src, int(sizeof(T)), g.nx, g.ny, g.nz, AXIS, box)) return cudaErrorNotSupported;
   const size_t smem = tma_smem_bytes<T, N, P>();
-  auto kern = tma_pass_kernel<T, N, AXIS, P, Store>;
+  auto kern = tma_pass_kernel<T, N, AXIS, P, Store, Mul>;
   static bool configured = false;   // per instantiation
   if (!configured) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -407,7 +439,7 @@ cudaError_t launch_tma_pass(const Geom& g, int kind, Tables<T> tb, const T* src,
   else tiles = g.ny * (g.nz / P);
   const int per_sm = smem * 2 <= 220 * 1024 ? 2 : 1;
   const int grid = tiles < per_sm * tma_config().sms ? tiles : per_sm * tma_config().sms;
-  kern<<<grid, tma_threads<T>(), smem, s>>>(map, g, kind, tb, st, tiles, tma_config().err);
+  kern<<<grid, tma_threads<T>(), smem, s>>>(map, g, kind, tb, st, tiles, tma_config().err, mul, dc1, dc2);
   return cudaGetLastError();
 }
 
@@ -467,6 +499,49 @@ cudaError_t launch_pass(const Geom& g, int kind, Tables<T> tb, LoadField<T> ld, 
 #undef QUASI_TMA_CASE
   }
   return launch_pass<T, AXIS, LoadField<T>, Store>(g, kind, tb, ld, st, s);
+}
+
+// x pass of an inverse transform whose input is mul(i,j,k) * src[i+di, j+dj, k]
+// (di, dj in {0, 1}; rows shifted past the end read as zero).  Falls back to
+// the general kernel with an equivalent loader when TMA is unavailable.
+template <typename T, class Mul>
+struct MulLoad {
+  Geom g;
+  const T* src;
+  Mul mul;
+  int di, dj;
+  __device__ T operator()(int i, int j, int k) const {
+    const int i1 = i + di, j1 = j + dj;
+    if (i1 >= g.nx || j1 >= g.ny) return T(0);
+    return T(double(src[lin(g, i1, j1, k)]) * mul(i, j, k));
+  }
+};
+
+template <typename T, class Mul, class Store>
+cudaError_t launch_mul_x_pass(const Geom& g, int kind, Tables<T> tb, const T* src, Mul mul, int di, int dj, Store st,
+                              cudaStream_t s) {
+  const long extent = g.nz;
+  if (tma_config().enabled && tma_config().err) {
+#define QUASI_TMA_CASE(NN)                                                                             \
+    case NN: {                                                                                         \
+      constexpr int P = pass_pencils<T>(NN);                                                           \
+      if (extent % P == 0) return launch_tma_pass<T, NN, 0, P>(g, kind, tb, src, st, s, mul, dj, di);  \
+      break;                                                                                           \
+    }
+    switch (g.nx) {
+      QUASI_TMA_CASE(16)
+      QUASI_TMA_CASE(32)
+      QUASI_TMA_CASE(64)
+      QUASI_TMA_CASE(96)
+      QUASI_TMA_CASE(128)
+      QUASI_TMA_CASE(192)
+      QUASI_TMA_CASE(256)
+      QUASI_TMA_CASE(512)
+      default: break;
+    }
+#undef QUASI_TMA_CASE
+  }
+  return launch_pass<T, 0>(g, kind, tb, MulLoad<T, Mul>{g, src, mul, di, dj}, st, s);
 }
 
 }  // namespace quasi

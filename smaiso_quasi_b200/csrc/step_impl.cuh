@@ -31,12 +31,19 @@ struct StepCtx {
   // captured graph per phase of the rotation), so the update writes its
   // result into a buffer nobody reads in that pass.
   T *psiq, *psiq_old, *psiq_new, *Nq, *Nq_old, *rhoq, *divvq, *Sx, *Sy, *Sz;
-  // real fields
-  T *psi, *psi_old, *rho, *rho_old, *vx, *vy, *vz, *divv, *p, *df, *lap;
+  // real fields (psi, psi_old and psi_new rotate through two buffers:
+  // psi_new is psi_old's buffer)
+  T *psi, *psi_old, *psi_new, *rho, *rho_old, *vx, *vy, *vz, *divv, *p, *df, *lap;
   T *gx, *gy, *gz, *rdx, *rdy, *rdz, *ldx, *ldy, *ldz, *sh, *dtpsi, *tmp;
 };
 
 __device__ __forceinline__ double sq(double x) { return x * x; }
+
+// Arithmetic type of the elementwise stages: the storage type.  The
+// semi-implicit update and the reductions always use double.
+template <typename T> using Arith = T;
+__device__ __forceinline__ double rcp(double x) { return __drcp_rn(x); }
+__device__ __forceinline__ float rcp(float x) { return __frcp_rn(x); }
 
 template <typename T>
 __device__ __forceinline__ size_t at(const StepCtx<T>& c, int i, int j, int k) { return lin(c.g, i, j, k); }
@@ -50,66 +57,60 @@ __device__ __forceinline__ double mq2c(const StepCtx<T>& c, int i, int j, int k)
 // Spectral loaders (first, x-axis pass of inverse transforms)
 // ---------------------------------------------------------------------------
 
-// dfDlapPsi = alpha (q0^2 - q^2) psiq                       quasi.cpp:1044
-template <typename T> struct LdDf {
+// ---------------------------------------------------------------------------
+// Spectral multipliers of the OUTPUT index (i, j, k) for the TMA x passes
+// (the loaders above, in the form the TMA pass applies them).
+// ---------------------------------------------------------------------------
+template <typename T> struct MDf {      // dfDlapPsi, quasi.cpp:1044
+  static constexpr bool kActive = true;
   StepCtx<T> c;
-  __device__ T operator()(int i, int j, int k) const {
-    return T(c.alpha * (c.q0 * c.q0 - mq2c(c, i, j, k)) * double(c.psiq[at(c, i, j, k)]));
-  }
+  __device__ double operator()(int i, int j, int k) const { return c.alpha * (c.q0 * c.q0 - mq2c(c, i, j, k)); }
 };
-
-// lapRhoDfDlapPsi = -q^2 dfDlapPsi                           quasi.cpp:1046-1047
-template <typename T> struct LdLap {
+template <typename T> struct MLap {     // lapRhoDfDlapPsi, quasi.cpp:1046-1047
+  static constexpr bool kActive = true;
   StepCtx<T> c;
-  __device__ T operator()(int i, int j, int k) const {
+  __device__ double operator()(int i, int j, int k) const {
     const double q2 = mq2c(c, i, j, k);
-    const double df = c.alpha * (c.q0 * c.q0 - q2) * double(c.psiq[at(c, i, j, k)]);
-    return T(-q2 * df);
+    return -q2 * (c.alpha * (c.q0 * c.q0 - q2));
   }
 };
-
-// sh = -aLin psiq,  aLin = ep - alpha (q0^2 - q^2)^2          quasi-stb.cpp:1019
-template <typename T> struct LdSh {
+template <typename T> struct MSh {      // -aLin, quasi-stb.cpp:1019
+  static constexpr bool kActive = true;
   StepCtx<T> c;
-  __device__ T operator()(int i, int j, int k) const {
+  __device__ double operator()(int i, int j, int k) const {
     const double q2 = mq2c(c, i, j, k);
-    const double alin = c.ep - c.alpha * sq(c.q0 * c.q0 - q2);
-    return T(-alin * double(c.psiq[at(c, i, j, k)]));
+    return -(c.ep - c.alpha * sq(c.q0 * c.q0 - q2));
   }
 };
-
-// Shifted spectral gradient along axis A: G[n] = -Vs[n] X[n+1], top index 0
-// (quasi.cpp:1120-1164).  LAP = true multiplies by -|q_s|^2 (quasi.cpp:1169-1186).
-template <typename T, int A, bool LAP> struct LdGrad {
+// Shifted gradient along A, quasi.cpp:1120-1186.  The input is read at
+// index + 1 along x or y by the TMA box offset (the row past the end reads as
+// zero: the reference's zero top DST index); along z the shift is applied
+// when storing (StShiftK), so the multiplier uses the output index k - 1.
+template <typename T, int A, bool LAP> struct MGrad {
+  static constexpr bool kActive = true;
   StepCtx<T> c;
-  const T* src;
-  __device__ T operator()(int i, int j, int k) const {
-    const int n = A == 0 ? i : (A == 1 ? j : k);
-    const int len = A == 0 ? c.g.nx : (A == 1 ? c.g.ny : c.g.nz);
-    if (n >= len - 1) return T(0);
-    const int i1 = i + (A == 0), j1 = j + (A == 1), k1 = k + (A == 2);
-    const double vs = A == 0 ? c.vsx[i] : (A == 1 ? c.vsy[j] : c.vsz[k]);
-    const double gval = -vs * double(src[at(c, i1, j1, k1)]);
-    if (!LAP) return T(gval);
+  __device__ double operator()(int i, int j, int k) const {
+    if (A == 2 && k == 0) return 0.0;
+    const int ko = A == 2 ? k - 1 : k;
+    const double vs = A == 0 ? c.vsx[i] : (A == 1 ? c.vsy[j] : c.vsz[ko]);
+    if (!LAP) return -vs;
     const double mq = (A == 0 ? sq(c.vsx[i]) : sq(c.vqx[i])) + (A == 1 ? sq(c.vsy[j]) : sq(c.vqy[j])) +
-                      (A == 2 ? sq(c.vsz[k]) : sq(c.vqz[k]));
-    return T(-mq * gval);
+                      (A == 2 ? sq(c.vsz[ko]) : sq(c.vqz[ko]));
+    return mq * vs;   // -mq * (-vs)
+  }
+};
+template <typename T> struct StShiftK {   // value of input k lands at k - 1; k = 0 zeroes nz - 1
+  Geom g;
+  T* dst;
+  __device__ void operator()(int i, int j, int k, T v) const {
+    if (k == 0) dst[lin(g, i, j, g.nz - 1)] = T(0);
+    else dst[lin(g, i, j, k - 1)] = v;
   }
 };
 
 // ---------------------------------------------------------------------------
 // Real-space loaders (first, z-axis pass of forward transforms)
 // ---------------------------------------------------------------------------
-
-// rho = kp sqrt(q0^2 psi^2 + |grad psi|^2) + rho_0          quasi.cpp:1243-1247
-template <typename T> struct LdRhoRaw {
-  StepCtx<T> c;
-  __device__ T operator()(int i, int j, int k) const {
-    const size_t id = at(c, i, j, k);
-    const double ps = c.psi[id], x = c.gx[id], y = c.gy[id], z = c.gz[id];
-    return T(c.kp * sqrt(c.q0 * c.q0 * ps * ps + x * x + y * y + z * z) + c.rho0);
-  }
-};
 
 template <typename T> struct LdRealField {
   StepCtx<T> c;
@@ -130,40 +131,45 @@ template <typename T> struct StRhoq {
   }
 };
 
-// psi_old <- psi, psi <- iCT(psiq')                           quasi.cpp:1961-1965
-template <typename T> struct StPsi {
-  StepCtx<T> c;
-  __device__ void operator()(int i, int j, int k, T v) const {
-    const size_t id = at(c, i, j, k);
-    c.psi_old[id] = c.psi[id];
-    c.psi[id] = v;
-  }
-};
-
 // ---------------------------------------------------------------------------
 // Elementwise stages.  Each reads every input field once, fully coalesced
 // (consecutive threads -> consecutive k), computes the terms shared by its
 // outputs once, and leaves the transforms around it plain.
 // ---------------------------------------------------------------------------
+// Iterate rows (i, j) with threads over k: one 32-bit division per row.
+#define QUASI_ROWS_BEGIN(g)                                                                       \
+  for (int row = blockIdx.x; row < (g).nx * (g).ny; row += gridDim.x) {                           \
+    const int i = row / (g).ny, j = row - i * (g).ny;                                             \
+    const size_t base = size_t(row) * (g).nz;                                                     \
+    for (int k = threadIdx.x; k < (g).nz; k += blockDim.x) {                                      \
+      const size_t id = base + k;
+#define QUASI_ROWS_END \
+  }                    \
+  }
+
+// rho = kp sqrt(q0^2 psi^2 + |grad psi|^2) + rho_0   quasi.cpp:1243-1247
 template <typename T>
-__device__ __forceinline__ void unlin(const Geom& g, size_t id, int& i, int& j, int& k) {
-  k = int(id % g.nz);
-  const size_t r = id / g.nz;
-  j = int(r % g.ny);
-  i = int(r / g.ny);
+__global__ void __launch_bounds__(256) rho_law_kernel(StepCtx<T> c, size_t n) {
+  using A = Arith<T>;
+  const A kp = A(c.kp), q02 = A(c.q0 * c.q0), r0 = A(c.rho0);
+  for (size_t id = blockIdx.x * size_t(blockDim.x) + threadIdx.x; id < n; id += size_t(gridDim.x) * blockDim.x) {
+    const A ps = c.psi[id], x = c.gx[id], y = c.gy[id], z = c.gz[id];
+    c.rho[id] = T(kp * sqrt(q02 * ps * ps + x * x + y * y + z * z) + r0);
+  }
 }
 
 // divv (after the switch) and rho_old <- rho          quasi.cpp:1273-1289
 template <typename T>
 __global__ void __launch_bounds__(256) divv_kernel(StepCtx<T> c, size_t n) {
+  using A = Arith<T>;
   const bool on = *c.nloop > c.divv_switch;
+  const A idt = A(1.0 / c.dt);
   for (size_t id = blockIdx.x * size_t(blockDim.x) + threadIdx.x; id < n; id += size_t(gridDim.x) * blockDim.x) {
-    const double r = c.rho[id];
+    const A r = c.rho[id];
     if (on) {
-      const double ro = c.rho_old[id];
-      const double adv = double(c.vx[id]) * double(c.rdx[id]) + double(c.vy[id]) * double(c.rdy[id]) +
-                         double(c.vz[id]) * double(c.rdz[id]);
-      c.divv[id] = T(-((r - ro) / c.dt + adv) / (0.5 * (r + ro)));
+      const A ro = c.rho_old[id];
+      const A adv = A(c.vx[id]) * A(c.rdx[id]) + A(c.vy[id]) * A(c.rdy[id]) + A(c.vz[id]) * A(c.rdz[id]);
+      c.divv[id] = T(-((r - ro) * idt + adv) / (A(0.5) * (r + ro)));
     }
     c.rho_old[id] = T(r);
   }
@@ -172,18 +178,20 @@ __global__ void __launch_bounds__(256) divv_kernel(StepCtx<T> c, size_t n) {
 // stress S (quasi.cpp:1305-1317) or mu grad psi (quasi-stb.cpp:1295-1305)
 template <typename T>
 __global__ void __launch_bounds__(256) stress_kernel(StepCtx<T> c, size_t n) {
+  using A = Arith<T>;
+  const A beta = A(c.beta), gamma = A(c.gamma);
   for (size_t id = blockIdx.x * size_t(blockDim.x) + threadIdx.x; id < n; id += size_t(gridDim.x) * blockDim.x) {
-    const double gx = c.gx[id], gy = c.gy[id], gz = c.gz[id];
+    const A gx = c.gx[id], gy = c.gy[id], gz = c.gz[id];
     if (c.variant == kQuasi) {
-      const double rho = c.rho[id];
-      const double lr = rho * double(c.lap[id]);
-      const double rd = rho * double(c.df[id]);
-      c.Sx[id] = T(lr * gx - rd * double(c.ldx[id]));
-      c.Sy[id] = T(lr * gy - rd * double(c.ldy[id]));
-      c.Sz[id] = T(lr * gz - rd * double(c.ldz[id]));
+      const A rho = c.rho[id];
+      const A lr = rho * A(c.lap[id]);
+      const A rd = rho * A(c.df[id]);
+      c.Sx[id] = T(lr * gx - rd * A(c.ldx[id]));
+      c.Sy[id] = T(lr * gy - rd * A(c.ldy[id]));
+      c.Sz[id] = T(lr * gz - rd * A(c.ldz[id]));
     } else {
-      const double ps = c.psi[id];
-      const double mu = double(c.sh[id]) - c.beta * ps * ps * ps + c.gamma * ps * ps * ps * ps * ps;
+      const A ps = c.psi[id];
+      const A mu = A(c.sh[id]) - beta * ps * ps * ps + gamma * ps * ps * ps * ps * ps;
       c.Sx[id] = T(mu * gx);
       c.Sy[id] = T(mu * gy);
       c.Sz[id] = T(mu * gz);
@@ -196,94 +204,94 @@ __global__ void __launch_bounds__(256) stress_kernel(StepCtx<T> c, size_t n) {
 // p^ -> p, v^ -> vx/vy/vz, scale*divv^ -> divv; the inverse transforms that
 // follow run in place on those fields.
 template <typename T>
-__global__ void __launch_bounds__(256) project_kernel(StepCtx<T> c, size_t n) {
+__global__ void __launch_bounds__(256) project_kernel(StepCtx<T> c) {
+  using A = Arith<T>;
   const Geom g = c.g;
-  for (size_t id = blockIdx.x * size_t(blockDim.x) + threadIdx.x; id < n; id += size_t(gridDim.x) * blockDim.x) {
-    int i, j, k;
-    unlin<T>(g, id, i, j, k);
-    const size_t sj = g.nz, si = size_t(g.ny) * g.nz;
-    const double qx = c.vqx[i], qy = c.vqy[j], qz = c.vqz[k];
-    const double sxc = c.Sx[id], syc = c.Sy[id], szc = c.Sz[id];
-    const double dvc = c.divvq[id];
+  const size_t sj = g.nz, si = size_t(g.ny) * g.nz;
+  const A scale = A(c.scale), nu = A(c.nu), inu = A(1.0 / c.nu);
+  QUASI_ROWS_BEGIN(g)
+    const A qx = A(c.vqx[i]), qy = A(c.vqy[j]), qz = A(c.vqz[k]);
+    const A sxc = c.Sx[id], syc = c.Sy[id], szc = c.Sz[id];
+    const A dvc = c.divvq[id];
     // p^: divergence of the stress shifted back onto the cosine grid
     {
       const bool on = c.variant == kQuasi ? (i + j + k != 0) : (i * j * k > 0);
-      double pv = 0.0;
+      A pv = A(0);
       if (on) {
-        const double sx = i > 0 ? double(c.Sx[id - si]) : 0.0;
-        const double sy = j > 0 ? double(c.Sy[id - sj]) : 0.0;
-        const double sz = k > 0 ? double(c.Sz[id - 1]) : 0.0;
-        const double q2 = qx * qx + qy * qy + qz * qz;
-        double v = -(qx * sx + qy * sy + qz * sz) / q2;
-        if (c.variant == kStb) v += c.nu * dvc;
-        pv = c.scale * v;
+        const A sx = i > 0 ? A(c.Sx[id - si]) : A(0);
+        const A sy = j > 0 ? A(c.Sy[id - sj]) : A(0);
+        const A sz = k > 0 ? A(c.Sz[id - 1]) : A(0);
+        A v = -(qx * sx + qy * sy + qz * sz) * rcp(qx * qx + qy * qy + qz * qz);
+        if (c.variant == kStb) v += nu * dvc;
+        pv = scale * v;
       }
       c.p[id] = T(pv);
     }
-    // v^x (i < nx-1)
+    // v^x (i < nx-1): CM1 = scale/(nu mq), CM2 = Vs/mq  (quasi.cpp:889-899)
     {
-      double v = 0.0;
+      A v = A(0);
       if (i < g.nx - 1) {
-        const double sy = j > 0 ? double(c.Sy[id + si - sj]) : 0.0;
-        const double sz = k > 0 ? double(c.Sz[id + si - 1]) : 0.0;
-        const double vs = c.vsx[i];
-        const double mq = vs * vs + qy * qy + qz * qz;
-        const double dot = vs * sxc + qy * sy + qz * sz;
-        v = (c.scale / (c.nu * mq)) * (sxc - (vs / mq) * dot + c.nu * vs * double(c.divvq[id + si]));
+        const A sy = j > 0 ? A(c.Sy[id + si - sj]) : A(0);
+        const A sz = k > 0 ? A(c.Sz[id + si - 1]) : A(0);
+        const A vs = A(c.vsx[i]);
+        const A inv = rcp(vs * vs + qy * qy + qz * qz);
+        const A dot = vs * sxc + qy * sy + qz * sz;
+        v = (scale * inv * inu) * (sxc - (vs * inv) * dot + nu * vs * A(c.divvq[id + si]));
       }
       c.vx[id] = T(v);
     }
     // v^y, v^z (j < ny-1, k < nz-1); Sx from the plane halo #4 delivers (quasi.cpp:1649)
-    double vy = 0.0, vz = 0.0;
+    A vy = A(0), vz = A(0);
     if (j < g.ny - 1 && k < g.nz - 1) {
       const int isrc = (i % c.n0 == 0) ? i - c.n0 : i - 1;
-      const size_t bx = size_t(isrc) * si + size_t(j) * sj + k;
+      const size_t bx = size_t(isrc < 0 ? 0 : isrc) * si + size_t(j) * sj + k;
       {
-        const double sx = i > 0 ? double(c.Sx[bx + sj]) : 0.0;
-        const double sz = k > 0 ? double(c.Sz[id + sj - 1]) : 0.0;
-        const double vs = c.vsy[j];
-        const double mq = qx * qx + vs * vs + qz * qz;
-        const double dot = qx * sx + vs * syc + qz * sz;
-        vy = (c.scale / (c.nu * mq)) * (syc - (vs / mq) * dot + c.nu * vs * double(c.divvq[id + sj]));
+        const A sx = i > 0 ? A(c.Sx[bx + sj]) : A(0);
+        const A sz = k > 0 ? A(c.Sz[id + sj - 1]) : A(0);
+        const A vs = A(c.vsy[j]);
+        const A inv = rcp(qx * qx + vs * vs + qz * qz);
+        const A dot = qx * sx + vs * syc + qz * sz;
+        vy = (scale * inv * inu) * (syc - (vs * inv) * dot + nu * vs * A(c.divvq[id + sj]));
       }
       {
-        const double sx = i > 0 ? double(c.Sx[bx + 1]) : 0.0;
-        const double sy = j > 0 ? double(c.Sy[id - sj + 1]) : 0.0;
-        const double vs = c.vsz[k];
-        const double mq = qx * qx + qy * qy + vs * vs;
-        const double dot = qx * sx + qy * sy + vs * szc;
-        vz = (c.scale / (c.nu * mq)) * (szc - (vs / mq) * dot + c.nu * vs * double(c.divvq[id + 1]));
+        const A sx = i > 0 ? A(c.Sx[bx + 1]) : A(0);
+        const A sy = j > 0 ? A(c.Sy[id - sj + 1]) : A(0);
+        const A vs = A(c.vsz[k]);
+        const A inv = rcp(qx * qx + qy * qy + vs * vs);
+        const A dot = qx * sx + qy * sy + vs * szc;
+        vz = (scale * inv * inu) * (szc - (vs * inv) * dot + nu * vs * A(c.divvq[id + 1]));
       }
     }
     c.vy[id] = T(vy);
     c.vz[id] = T(vz);
-    if (c.variant == kQuasi) c.divv[id] = T(c.scale * dvc);
-  }
+    if (c.variant == kQuasi) c.divv[id] = T(scale * dvc);
+  QUASI_ROWS_END
 }
 
 // Nonlinear term N (quasi.cpp:1905-1929, quasi-stb.cpp:1900-1924) -> Nq
 template <typename T>
 __global__ void __launch_bounds__(256) nonlinear_kernel(StepCtx<T> c, size_t n) {
+  using A = Arith<T>;
   const bool pcoup = *c.nloop > c.divv_switch + 1;
+  const A ep = A(c.ep), beta = A(c.beta), gamma = A(c.gamma), cp = A(c.kp / (c.rho_s * c.rho_s));
   for (size_t id = blockIdx.x * size_t(blockDim.x) + threadIdx.x; id < n; id += size_t(gridDim.x) * blockDim.x) {
-    const double ps = c.psi[id];
-    const double p3 = ps * ps * ps, p5 = p3 * ps * ps;
-    const double adv = double(c.vx[id]) * double(c.gx[id]) + double(c.vy[id]) * double(c.gy[id]) +
-                       double(c.vz[id]) * double(c.gz[id]);
-    double nv;
+    const A ps = c.psi[id];
+    const A p3 = ps * ps * ps, p5 = p3 * ps * ps;
+    const A adv = A(c.vx[id]) * A(c.gx[id]) + A(c.vy[id]) * A(c.gy[id]) + A(c.vz[id]) * A(c.gz[id]);
+    A nv;
     if (c.variant == kQuasi) {
-      const double rho = c.rho[id];
-      nv = rho * (c.ep * ps - double(c.df[id]) + c.beta * p3 - c.gamma * p5) - rho * double(c.lap[id]) - adv;
+      const A rho = c.rho[id];
+      nv = rho * (ep * ps - A(c.df[id]) + beta * p3 - gamma * p5) - rho * A(c.lap[id]) - adv;
       if (pcoup) {
-        const double a = c.rdx[id], b = c.rdy[id], d = c.rdz[id];
-        nv += double(c.p[id]) * c.kp * sqrt(a * a + b * b + d * d) / (c.rho_s * c.rho_s);
+        const A a = c.rdx[id], b = c.rdy[id], d = c.rdz[id];
+        nv += A(c.p[id]) * cp * sqrt(a * a + b * b + d * d);
       }
     } else {
       if (c.store_dtpsi) {
-        const double mu = double(c.sh[id]) - c.beta * p3 + c.gamma * p5;
+        const A mu = A(c.sh[id]) - beta * p3 + gamma * p5;
         c.dtpsi[id] = T(-mu - adv);   // quasi-stb.cpp:1909-1912, rho == 1
       }
-      nv = c.beta * p3 - c.gamma * p5 - adv;
+      nv = beta * p3 - gamma * p5 - adv;
     }
     c.Nq[id] = T(nv);
   }
@@ -291,18 +299,16 @@ __global__ void __launch_bounds__(256) nonlinear_kernel(StepCtx<T> c, size_t n) 
 
 // Semi-implicit update -> psiq_new (quasi.cpp:1944-1962, quasi-stb.cpp:1946-1958)
 template <typename T>
-__global__ void __launch_bounds__(256) update_kernel(StepCtx<T> c, size_t n) {
+__global__ void __launch_bounds__(256) update_kernel(StepCtx<T> c) {
   const Geom g = c.g;
   const bool first = *c.nloop == 1;
-  for (size_t id = blockIdx.x * size_t(blockDim.x) + threadIdx.x; id < n; id += size_t(gridDim.x) * blockDim.x) {
-    int i, j, k;
-    unlin<T>(g, id, i, j, k);
+  const double dtd2 = c.dt / 2;
+  QUASI_ROWS_BEGIN(g)
     const double q2 = mq2c(c, i, j, k);
     const double alin = c.ep - c.alpha * sq(c.q0 * c.q0 - q2);
     const double pq = c.psiq[id];
     const double nq = c.Nq[id];
     const double nq_old = first ? nq : double(c.Nq_old[id]);   // :1936-1938
-    const double dtd2 = c.dt / 2;
     double nv;
     if (c.variant == kQuasi) {
       const double c1 = 2.0 - c.dt * c.rho_m * alin, c2 = 1.5 - c.dt * c.rho_m * alin;   // :886-887
@@ -312,7 +318,7 @@ __global__ void __launch_bounds__(256) update_kernel(StepCtx<T> c, size_t n) {
       nv = (c1 * pq + dtd2 * c.scale * (3.0 * nq - nq_old)) / c2;
     }
     c.psiq_new[id] = T(nv);
-  }
+  QUASI_ROWS_END
 }
 
 // ---------------------------------------------------------------------------
@@ -332,6 +338,18 @@ cudaError_t inverse3(const Geom& g, const AxisTables<T>& tb, const int kinds[3],
   if ((e = launch_pass<T, 1>(g, kinds[1], tb.t[1], LoadField<T>{g, dst}, StoreField<T>{g, dst}, s)) != cudaSuccess)
     return e;
   return launch_pass<T, 2>(g, kinds[2], tb.t[2], LoadField<T>{g, dst}, st, s);
+}
+
+// Inverse with a spectral multiplier: x pass on mul * src[shifted] -> dst
+// through stx, then plain y and z passes in place.
+template <typename T, class Mul, class StX>
+cudaError_t inverse3_mul(const Geom& g, const AxisTables<T>& tb, const int kinds[3], const T* src, Mul mul, int di,
+                         int dj, StX stx, T* dst, cudaStream_t s) {
+  cudaError_t e;
+  if ((e = launch_mul_x_pass<T>(g, kinds[0], tb.t[0], src, mul, di, dj, stx, s)) != cudaSuccess) return e;
+  if ((e = launch_pass<T, 1>(g, kinds[1], tb.t[1], LoadField<T>{g, dst}, StoreField<T>{g, dst}, s)) != cudaSuccess)
+    return e;
+  return launch_pass<T, 2>(g, kinds[2], tb.t[2], LoadField<T>{g, dst}, StoreField<T>{g, dst}, s);
 }
 
 // Forward: z pass (loader -> dst), y pass, x pass (storer).
@@ -376,20 +394,22 @@ cudaError_t enqueue_step(const StepCtx<T>& c, const AxisTables<T>& tb, int* nloo
   auto ld = [&](T* d) { return LoadField<T>{g, d}; };
   if (c.variant == kQuasi) {
     // a3 prologue quasi.cpp:1036-1057
-    QUASI_TRY(inverse3(g, tb, kiCT, LdDf<T>{c}, c.df, st(c.df), s));
-    QUASI_TRY(inverse3(g, tb, kiCT, LdLap<T>{c}, c.lap, st(c.lap), s));
+    QUASI_TRY(inverse3_mul(g, tb, kiCT, c.psiq, MDf<T>{c}, 0, 0, st(c.df), c.df, s));
+    QUASI_TRY(inverse3_mul(g, tb, kiCT, c.psiq, MLap<T>{c}, 0, 0, st(c.lap), c.lap, s));
     // a4 gradients quasi.cpp:1120-1232
-    QUASI_TRY(inverse3(g, tb, kiSTx, LdGrad<T, 0, false>{c, c.psiq}, c.gx, st(c.gx), s));
-    QUASI_TRY(inverse3(g, tb, kiSTy, LdGrad<T, 1, false>{c, c.psiq}, c.gy, st(c.gy), s));
-    QUASI_TRY(inverse3(g, tb, kiSTz, LdGrad<T, 2, false>{c, c.psiq}, c.gz, st(c.gz), s));
-    QUASI_TRY(inverse3(g, tb, kiSTx, LdGrad<T, 0, false>{c, c.rhoq}, c.rdx, st(c.rdx), s));
-    QUASI_TRY(inverse3(g, tb, kiSTy, LdGrad<T, 1, false>{c, c.rhoq}, c.rdy, st(c.rdy), s));
-    QUASI_TRY(inverse3(g, tb, kiSTz, LdGrad<T, 2, false>{c, c.rhoq}, c.rdz, st(c.rdz), s));
-    QUASI_TRY(inverse3(g, tb, kiSTx, LdGrad<T, 0, true>{c, c.psiq}, c.ldx, st(c.ldx), s));
-    QUASI_TRY(inverse3(g, tb, kiSTy, LdGrad<T, 1, true>{c, c.psiq}, c.ldy, st(c.ldy), s));
-    QUASI_TRY(inverse3(g, tb, kiSTz, LdGrad<T, 2, true>{c, c.psiq}, c.ldz, st(c.ldz), s));
+    QUASI_TRY(inverse3_mul(g, tb, kiSTx, c.psiq, MGrad<T, 0, false>{c}, 1, 0, st(c.gx), c.gx, s));
+    QUASI_TRY(inverse3_mul(g, tb, kiSTy, c.psiq, MGrad<T, 1, false>{c}, 0, 1, st(c.gy), c.gy, s));
+    QUASI_TRY(inverse3_mul(g, tb, kiSTz, c.psiq, MGrad<T, 2, false>{c}, 0, 0, StShiftK<T>{g, c.gz}, c.gz, s));
+    QUASI_TRY(inverse3_mul(g, tb, kiSTx, c.rhoq, MGrad<T, 0, false>{c}, 1, 0, st(c.rdx), c.rdx, s));
+    QUASI_TRY(inverse3_mul(g, tb, kiSTy, c.rhoq, MGrad<T, 1, false>{c}, 0, 1, st(c.rdy), c.rdy, s));
+    QUASI_TRY(inverse3_mul(g, tb, kiSTz, c.rhoq, MGrad<T, 2, false>{c}, 0, 0, StShiftK<T>{g, c.rdz}, c.rdz, s));
+    QUASI_TRY(inverse3_mul(g, tb, kiSTx, c.psiq, MGrad<T, 0, true>{c}, 1, 0, st(c.ldx), c.ldx, s));
+    QUASI_TRY(inverse3_mul(g, tb, kiSTy, c.psiq, MGrad<T, 1, true>{c}, 0, 1, st(c.ldy), c.ldy, s));
+    QUASI_TRY(inverse3_mul(g, tb, kiSTz, c.psiq, MGrad<T, 2, true>{c}, 0, 0, StShiftK<T>{g, c.ldz}, c.ldz, s));
     // a5 density + filter quasi.cpp:1237-1268 (rho doubles as the scratch)
-    QUASI_TRY(forward3(g, tb, kCT, LdRhoRaw<T>{c}, c.rho, StRhoq<T>{c}, s));
+    rho_law_kernel<T><<<kEwBlocks, 256, 0, s>>>(c, n);
+    QUASI_TRY(cudaGetLastError());
+    QUASI_TRY(forward3(g, tb, kCT, ld(c.rho), c.rho, StRhoq<T>{c}, s));
     QUASI_TRY(inverse3(g, tb, kiCT, ld(c.rhoq), c.rho, st(c.rho), s));
     // a6 divv quasi.cpp:1273-1293
     divv_kernel<T><<<kEwBlocks, 256, 0, s>>>(c, n);
@@ -397,10 +417,10 @@ cudaError_t enqueue_step(const StepCtx<T>& c, const AxisTables<T>& tb, int* nloo
     QUASI_TRY(forward3(g, tb, kCT, ld(c.divv), c.divvq, st(c.divvq), s));
   } else {
     // quasi-stb.cpp:1005-1038 (the unused dRho transform is elided)
-    QUASI_TRY(inverse3(g, tb, kiCT, LdSh<T>{c}, c.sh, st(c.sh), s));
-    QUASI_TRY(inverse3(g, tb, kiSTx, LdGrad<T, 0, false>{c, c.psiq}, c.gx, st(c.gx), s));
-    QUASI_TRY(inverse3(g, tb, kiSTy, LdGrad<T, 1, false>{c, c.psiq}, c.gy, st(c.gy), s));
-    QUASI_TRY(inverse3(g, tb, kiSTz, LdGrad<T, 2, false>{c, c.psiq}, c.gz, st(c.gz), s));
+    QUASI_TRY(inverse3_mul(g, tb, kiCT, c.psiq, MSh<T>{c}, 0, 0, st(c.sh), c.sh, s));
+    QUASI_TRY(inverse3_mul(g, tb, kiSTx, c.psiq, MGrad<T, 0, false>{c}, 1, 0, st(c.gx), c.gx, s));
+    QUASI_TRY(inverse3_mul(g, tb, kiSTy, c.psiq, MGrad<T, 1, false>{c}, 0, 1, st(c.gy), c.gy, s));
+    QUASI_TRY(inverse3_mul(g, tb, kiSTz, c.psiq, MGrad<T, 2, false>{c}, 0, 0, StShiftK<T>{g, c.gz}, c.gz, s));
     // rho == 1, divv == 0, grad rho == 0 (rhoq never leaves 0): quasi-stb.cpp:1232
   }
   // a7 stress quasi.cpp:1298-1330
@@ -410,7 +430,7 @@ cudaError_t enqueue_step(const StepCtx<T>& c, const AxisTables<T>& tb, int* nloo
   QUASI_TRY(forward3(g, tb, kSTy, ld(c.Sy), c.Sy, st(c.Sy), s));
   QUASI_TRY(forward3(g, tb, kSTz, ld(c.Sz), c.Sz, st(c.Sz), s));
   // a8 pressure, a9 velocity, a10 scaled divv quasi.cpp:1336-1900
-  project_kernel<T><<<kEwBlocks, 256, 0, s>>>(c, n);
+  project_kernel<T><<<kEwBlocks, 256, 0, s>>>(c);
   QUASI_TRY(cudaGetLastError());
   if (c.variant == kQuasi) QUASI_TRY(inverse3(g, tb, kiCT, ld(c.p), c.p, st(c.p), s));
   QUASI_TRY(inverse3(g, tb, kiSTx, ld(c.vx), c.vx, st(c.vx), s));
@@ -422,9 +442,9 @@ cudaError_t enqueue_step(const StepCtx<T>& c, const AxisTables<T>& tb, int* nloo
   QUASI_TRY(cudaGetLastError());
   QUASI_TRY(forward3(g, tb, kCT, ld(c.Nq), c.Nq, st(c.Nq), s));
   // a12 update + iCT quasi.cpp:1944-1965
-  update_kernel<T><<<kEwBlocks, 256, 0, s>>>(c, n);
+  update_kernel<T><<<kEwBlocks, 256, 0, s>>>(c);
   QUASI_TRY(cudaGetLastError());
-  QUASI_TRY(inverse3(g, tb, kiCT, ld(c.psiq_new), c.tmp, StPsi<T>{c}, s));
+  QUASI_TRY(inverse3(g, tb, kiCT, ld(c.psiq_new), c.tmp, st(c.psi_new), s));   // psi_old <- psi by rotation
   return cudaSuccess;
 }
 
@@ -444,7 +464,7 @@ template <typename T>
 __global__ void init_state_kernel(StepCtx<T> c, size_t n) {
   for (size_t id = blockIdx.x * size_t(blockDim.x) + threadIdx.x; id < n; id += size_t(gridDim.x) * blockDim.x) {
     c.psiq_old[id] = c.psiq[id];   // quasi.cpp:939
-    c.psi_old[id] = c.psi[id];
+    c.psi_old[id] = c.psi[id];   // quasi.cpp:948
     c.divv[id] = T(0);
     c.divvq[id] = T(0);
     c.rhoq[id] = T(0);
