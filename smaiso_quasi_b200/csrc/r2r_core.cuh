@@ -65,6 +65,13 @@ QHD constexpr RadixPlan radix_plan(int n) {
 
 QHD constexpr bool size_supported(int n) { return n >= 4 && (n % 2) == 0 && radix_plan(n).n_stages > 0; }
 
+// Stride s (product of the radices before stage st) and sub-length n = N / s.
+QHD constexpr int stage_stride(int n, int st) {
+  int s = 1;
+  for (int i = 0; i < st; ++i) s *= radix_plan(n).r[i];
+  return s;
+}
+
 // ---------------------------------------------------------------------------
 // Small forward DFT codelets, exp(-2 pi i tu / R)
 // ---------------------------------------------------------------------------
@@ -247,10 +254,10 @@ struct TileFFT {
     Cx<T> v[per_thread<R>()][R];
   };
 
-  template <int R, class Src>
-  QHD static void stage_read(int tid, const Cx<T>* cb, const Src& src, int kind, int n, int s, bool first,
-                             Tables<T> tb, StageRegs<R>& r) {
-    const int m = n / R;
+  template <int R, int n, int s, class Src>
+  QHD static void stage_read(int tid, const Cx<T>* cb, const Src& src, int kind, bool first, Tables<T> tb,
+                             StageRegs<R>& r) {
+    constexpr int m = n / R;
 #pragma unroll
     for (int c = 0; c < per_thread<R>(); ++c) {
       const int w = tid + c * NT;
@@ -270,9 +277,8 @@ struct TileFFT {
     }
   }
 
-  template <int R, class Snk>
-  QHD static void stage_write(int tid, Cx<T>* cb, const Snk& snk, int kind, int s, bool last,
-                              const StageRegs<R>& r) {
+  template <int R, int s, class Snk>
+  QHD static void stage_write(int tid, Cx<T>* cb, const Snk& snk, int kind, bool last, const StageRegs<R>& r) {
 #pragma unroll
     for (int c = 0; c < per_thread<R>(); ++c) {
       const int w = tid + c * NT;
@@ -354,11 +360,12 @@ struct NoHook {
 // `hook()` runs on every thread right after the first stage's closing barrier
 // (the moment the first stage's input is no longer needed).
 template <typename T, int N, int G, int NT, int ST, bool INPLACE, class Exec, class Src, class Snk, class Hook>
-QHD void r2r_stages(Exec& ex, int tid, int kind, Cx<T>* cb, const Src& src, const Snk& snk, Tables<T> tb, int n,
-                    int s, const Hook& hook) {
+QHD void r2r_stages(Exec& ex, int tid, int kind, Cx<T>* cb, const Src& src, const Snk& snk, Tables<T> tb,
+                    const Hook& hook) {
   using F = TileFFT<T, N, G, NT>;
   if constexpr (ST < F::plan.n_stages) {
     constexpr int R = F::plan.r[ST];
+    constexpr int s = stage_stride(N, ST), n = N / s;
     constexpr bool first = ST == 0, last = ST == F::plan.n_stages - 1;
     using Regs = typename F::template StageRegs<R>;
     Regs regs;
@@ -371,14 +378,14 @@ QHD void r2r_stages(Exec& ex, int tid, int kind, Cx<T>* cb, const Src& src, cons
     // a write half must be visible before the next read half; an inverse
     // kind's last stage writing to global memory is followed by nothing
     const bool after = !last || is_forward(kind) || INPLACE;
-    ex.phase([&](int t, Regs& rg) { F::template stage_read<R>(t, cb, src, kind, n, s, first, tb, rg); },
-             [&](int t, Regs& rg) { F::template stage_write<R>(t, cb, snk, kind, s, last, rg); }, tid, regs, mid,
+    ex.phase([&](int t, Regs& rg) { F::template stage_read<R, n, s>(t, cb, src, kind, first, tb, rg); },
+             [&](int t, Regs& rg) { F::template stage_write<R, s>(t, cb, snk, kind, last, rg); }, tid, regs, mid,
              after);
     if constexpr (first) {
       if (!after) ex.sync();   // the hook may recycle the first stage's input
       hook();
     }
-    r2r_stages<T, N, G, NT, ST + 1, INPLACE>(ex, tid, kind, cb, src, snk, tb, n / R, s * R, hook);
+    r2r_stages<T, N, G, NT, ST + 1, INPLACE>(ex, tid, kind, cb, src, snk, tb, hook);
   }
 }
 
@@ -386,7 +393,7 @@ template <typename T, int N, int G, int NT, bool INPLACE, class Exec, class Src,
 QHD void r2r_tile(Exec& ex, int tid, int kind, Cx<T>* cb, const Src& src, const Snk& snk, Tables<T> tb,
                   const Hook& hook = Hook()) {
   using F = TileFFT<T, N, G, NT>;
-  r2r_stages<T, N, G, NT, 0, INPLACE>(ex, tid, kind, cb, src, snk, tb, N, 1, hook);
+  r2r_stages<T, N, G, NT, 0, INPLACE>(ex, tid, kind, cb, src, snk, tb, hook);
   if (is_forward(kind)) {
     typename F::UnpackRegs regs;
     ex.phase([&](int t, typename F::UnpackRegs& rg) { F::unpack_read(t, cb, tb, rg); },
