@@ -147,6 +147,23 @@ QUASI_API int quasi_growth_rate(quasi_handle* h, double* out);
 QUASI_API int quasi_save(quasi_handle* h, const char* path);
 QUASI_API int quasi_load(quasi_handle* h, const char* path);
 
+/* ---- diagnostics without allocation --------------------------------------
+ * No counterpart in the reference (its reductions are plain host loops).
+ * The same FP64 reductions as quasi_diagnostics, for callers that cannot
+ * call cudaMalloc (a device whose memory is owned by another component's
+ * pool, a real-time host loop that must not synchronise on an allocation):
+ * no handle, nothing allocated; the caller passes its own device fields
+ * (nx*ny*nz elements of cfg->precision's type, reference layout) and a host
+ * array for the 3 results, and may pass a cudaStream_t (NULL: the default
+ * stream); the call returns after the results are on the host.  The partial
+ * sums live in a fixed __device__ array of 64 KiB that every GPU loading the
+ * library keeps until exit, so grids are limited to 2^25 cells (larger ones
+ * are rejected).  The first call on a device looks that array up; make it
+ * before any stream capture.  Calls that overlap on the GPU race.
+ * df may be NULL for the quasi-stb variant (no energy). */
+QUASI_API int quasi_diagnostics_noalloc(const quasi_config* cfg, const void* psi, const void* psi_old,
+                                        const void* rho, const void* df, double out[3], void* stream);
+
 /* ---- seeded initial conditions (host only, no device needed) -----------
  * The reference builds a focal-conic domain (quasi.cpp:543-589) or reads psi
  * from text (quasi.cpp:692-717); the workloads add planar, undulated,

@@ -25,7 +25,7 @@ DRIVER = PKG / "quasi_run"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
            "-Xcompiler", "-fvisibility=hidden", "-I", str(ROOT / "include")]
-UNITS = ["abi.cu", "r2r_api.cu", "engine_f64.cu", "engine_f32.cu", "ic.cpp"]
+UNITS = ["abi.cu", "r2r_api.cu", "engine_f64.cu", "engine_f32.cu", "ic.cpp", "noalloc.cu"]
 
 
 def nvcc() -> str:
