@@ -155,7 +155,7 @@ __global__ void __launch_bounds__(pass_threads<T>(), pass_min_blocks<T>()) axis_
                                                                       Store st) {
   constexpr int NT = pass_threads<T>();
   constexpr int LD = tile_ld(N);
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   T* buf = reinterpret_cast<T*>(smem_raw);
   const int tile = blockIdx.x;
   const int tid = threadIdx.x;
