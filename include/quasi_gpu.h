@@ -126,6 +126,14 @@ QUASI_API int quasi_step_kernels(quasi_handle* h, int* launches);
  * with CUDA events; operates on a scratch field.  For roofline reporting. */
 QUASI_API int quasi_time_axis_pass(quasi_handle* h, int axis, int reps, double* avg_ms);
 
+/* Enqueue nsteps steps on the handle's stream and return at once, so that
+ * several handles (an ensemble of instances) run concurrently on one GPU;
+ * quasi_synchronize waits for them and reports any device-side error.
+ * Every other call of a handle synchronises by itself.  No reference
+ * counterpart (the reference runs one instance per MPI job). */
+QUASI_API int quasi_step_async(quasi_handle* h, int nsteps);
+QUASI_API int quasi_synchronize(quasi_handle* h);
+
 /* Steps taken since quasi_init (the reference's nLoop). */
 QUASI_API int quasi_step_count(const quasi_handle* h, long* nloop);
 

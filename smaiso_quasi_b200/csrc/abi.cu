@@ -138,6 +138,10 @@ int quasi_init(quasi_handle* h) { QUASI_CALL(h, h->eng->init()); }
 
 int quasi_step(quasi_handle* h, int nsteps) { QUASI_CALL(h, h->eng->step(nsteps, nullptr)); }
 
+int quasi_step_async(quasi_handle* h, int nsteps) { QUASI_CALL(h, h->eng->step_async(nsteps)); }
+
+int quasi_synchronize(quasi_handle* h) { QUASI_CALL(h, h->eng->synchronize()); }
+
 int quasi_step_timed(quasi_handle* h, int nsteps, double* device_ms) {
   if (!device_ms) return fail(QUASI_ERR_INVALID, "null device_ms");
   QUASI_CALL(h, h->eng->step(nsteps, device_ms));

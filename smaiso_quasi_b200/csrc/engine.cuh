@@ -20,6 +20,8 @@ class EngineBase {
   virtual int set_psi(const double* host) = 0;
   virtual int init() = 0;
   virtual int step(int nsteps, double* device_ms) = 0;
+  virtual int step_async(int nsteps) = 0;
+  virtual int synchronize() = 0;
   virtual int get_field(int field, double* host) = 0;
   virtual int diagnostics(double out[3]) = 0;
   virtual int growth_rate(double* out) = 0;

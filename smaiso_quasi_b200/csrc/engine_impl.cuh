@@ -147,27 +147,25 @@ class Engine : public EngineBase {
   }
 
   int step(int nsteps, double* device_ms) override {
-    if (!initialized_) { err = "quasi_step before quasi_init"; return QUASI_ERR_STATE; }
-    if (nsteps < 0) { err = "nsteps < 0"; return QUASI_ERR_INVALID; }
-    if (!graph_exec_[0]) {
-      int rc = capture();
-      if (rc) return rc;
-    }
-    if (device_ms && !cuda_ok(cudaEventRecord(ev0_, stream_), "event")) return QUASI_ERR_CUDA;
-    for (int s = 0; s < nsteps; ++s)
-      if (!cuda_ok(cudaGraphLaunch(graph_exec_[(nloop_ + s) % kPhases], stream_), "graph launch"))
-        return QUASI_ERR_CUDA;
-    if (device_ms && !cuda_ok(cudaEventRecord(ev1_, stream_), "event")) return QUASI_ERR_CUDA;
-    if (!cuda_ok(cudaStreamSynchronize(stream_), "step sync")) return QUASI_ERR_CUDA;
-    int tma_failed = 0;
-    if (!cuda_ok(cudaMemcpy(&tma_failed, tma_err_, sizeof(int), cudaMemcpyDeviceToHost), "flag")) return QUASI_ERR_CUDA;
-    if (tma_failed) { err = "a tile copy did not complete within its wait limit"; return QUASI_ERR_CUDA; }
+    int rc = enqueue(nsteps, device_ms != nullptr);
+    if (rc) return rc;
+    rc = synchronize();
+    if (rc) return rc;
     if (device_ms) {
       float ms = 0;
       if (!cuda_ok(cudaEventElapsedTime(&ms, ev0_, ev1_), "elapsed")) return QUASI_ERR_CUDA;
       *device_ms = ms;
     }
-    nloop_ += nsteps;
+    return QUASI_OK;
+  }
+
+  int step_async(int nsteps) override { return enqueue(nsteps, false); }
+
+  int synchronize() override {
+    if (!cuda_ok(cudaStreamSynchronize(stream_), "step sync")) return QUASI_ERR_CUDA;
+    int tma_failed = 0;
+    if (!cuda_ok(cudaMemcpy(&tma_failed, tma_err_, sizeof(int), cudaMemcpyDeviceToHost), "flag")) return QUASI_ERR_CUDA;
+    if (tma_failed) { err = "a tile copy did not complete within its wait limit"; return QUASI_ERR_CUDA; }
     return QUASI_OK;
   }
 
@@ -301,6 +299,24 @@ class Engine : public EngineBase {
     h.nloop = nloop_;
     return h;
   }
+  // Launch the step graphs of nsteps steps on the handle's stream (the host
+  // step counter advances at once; the device one as the graphs run).
+  int enqueue(int nsteps, bool timed) {
+    if (!initialized_) { err = "quasi_step before quasi_init"; return QUASI_ERR_STATE; }
+    if (nsteps < 0) { err = "nsteps < 0"; return QUASI_ERR_INVALID; }
+    if (!graph_exec_[0]) {
+      int rc = capture();
+      if (rc) return rc;
+    }
+    if (timed && !cuda_ok(cudaEventRecord(ev0_, stream_), "event")) return QUASI_ERR_CUDA;
+    for (int s = 0; s < nsteps; ++s)
+      if (!cuda_ok(cudaGraphLaunch(graph_exec_[(nloop_ + s) % kPhases], stream_), "graph launch"))
+        return QUASI_ERR_CUDA;
+    if (timed && !cuda_ok(cudaEventRecord(ev1_, stream_), "event")) return QUASI_ERR_CUDA;
+    nloop_ += nsteps;
+    return QUASI_OK;
+  }
+
   // the state a step reads (at the phase set by set_phase(nloop))
   std::vector<T*> carried() {
     return {c_.psiq, c_.psiq_old, c_.Nq_old, c_.rhoq, c_.rho_old, c_.rho, c_.vx, c_.vy, c_.vz,

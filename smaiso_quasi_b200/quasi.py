@@ -36,6 +36,7 @@ EXPORTS = [
     "quasi_diagnostics", "quasi_growth_rate", "quasi_save", "quasi_load", "quasi_r2r_plan_create",
     "quasi_r2r_execute_device", "quasi_r2r_execute_host", "quasi_r2r_plan_destroy",
     "quasi_ic_default", "quasi_initial_condition", "quasi_step_kernels", "quasi_time_axis_pass",
+    "quasi_step_async", "quasi_synchronize", "quasi_diagnostics_noalloc",
 ]
 IC_KIND = {"planar": 0, "undulated": 1, "interface": 2, "droplet": 3, "stb": 4, "focal_conic": 5}
 
@@ -89,6 +90,8 @@ def lib() -> ctypes.CDLL:
         L.quasi_init.argtypes = [ctypes.c_void_p]
         L.quasi_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.quasi_step_timed.argtypes = [ctypes.c_void_p, ctypes.c_int, dp]
+        L.quasi_step_async.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.quasi_synchronize.argtypes = [ctypes.c_void_p]
         L.quasi_step_count.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_long)]
         L.quasi_get_field.argtypes = [ctypes.c_void_p, ctypes.c_int, dp]
         L.quasi_diagnostics.argtypes = [ctypes.c_void_p, dp]
@@ -176,6 +179,13 @@ class Simulation:
 
     def step(self, n: int = 1) -> None:
         _check(lib().quasi_step(self._h, int(n)))
+
+    def step_async(self, n: int = 1) -> None:
+        """Enqueue n steps and return (see synchronize)."""
+        _check(lib().quasi_step_async(self._h, int(n)))
+
+    def synchronize(self) -> None:
+        _check(lib().quasi_synchronize(self._h))
 
     def step_timed(self, n: int) -> float:
         ms = ctypes.c_double()
