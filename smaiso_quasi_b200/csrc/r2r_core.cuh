@@ -50,11 +50,11 @@ struct RadixPlan {
   int r[6];
 };
 
-QHD constexpr RadixPlan radix_plan(int n) {
+QHD constexpr RadixPlan radix_plan(int n, int max_radix = 16) {
   RadixPlan p{0, {0, 0, 0, 0, 0, 0}};
   int m = n;
-  // prefer 16 and 8 (fewer stages), keep the 3s last
-  while (m % 16 == 0 && m != 32 && p.n_stages < 6) { p.r[p.n_stages++] = 16; m /= 16; }
+  // prefer the largest radix allowed (fewer stages), keep the 3s last
+  while (max_radix >= 16 && m % 16 == 0 && m != 32 && p.n_stages < 6) { p.r[p.n_stages++] = 16; m /= 16; }
   while (m % 8 == 0 && p.n_stages < 6) { p.r[p.n_stages++] = 8; m /= 8; }
   while (m % 4 == 0 && p.n_stages < 6) { p.r[p.n_stages++] = 4; m /= 4; }
   while (m % 2 == 0 && p.n_stages < 6) { p.r[p.n_stages++] = 2; m /= 2; }
@@ -66,11 +66,15 @@ QHD constexpr RadixPlan radix_plan(int n) {
 QHD constexpr bool size_supported(int n) { return n >= 4 && (n % 2) == 0 && radix_plan(n).n_stages > 0; }
 
 // Stride s (product of the radices before stage st) and sub-length n = N / s.
-QHD constexpr int stage_stride(int n, int st) {
+QHD constexpr int stage_stride(int n, int st, int max_radix) {
   int s = 1;
-  for (int i = 0; i < st; ++i) s *= radix_plan(n).r[i];
+  for (int i = 0; i < st; ++i) s *= radix_plan(n, max_radix).r[i];
   return s;
 }
+
+// Largest radix per element type: a radix-16 butterfly holds 16 complex values
+// in registers (64 registers in double), so double stops at 8.
+template <typename T> QHD constexpr int max_radix() { return sizeof(T) == 8 ? 8 : 16; }
 
 // ---------------------------------------------------------------------------
 // Small forward DFT codelets, exp(-2 pi i tu / R)
@@ -215,7 +219,7 @@ struct SmemSnk {
 
 template <typename T, int N, int G, int NT>
 struct TileFFT {
-  static constexpr RadixPlan plan = radix_plan(N);
+  static constexpr RadixPlan plan = radix_plan(N, max_radix<T>());
   static constexpr int LD = tile_ld(N);
   static_assert(plan.n_stages > 0, "unsupported transform length");
 
@@ -365,7 +369,7 @@ QHD void r2r_stages(Exec& ex, int tid, int kind, Cx<T>* cb, const Src& src, cons
   using F = TileFFT<T, N, G, NT>;
   if constexpr (ST < F::plan.n_stages) {
     constexpr int R = F::plan.r[ST];
-    constexpr int s = stage_stride(N, ST), n = N / s;
+    constexpr int s = stage_stride(N, ST, max_radix<T>()), n = N / s;
     constexpr bool first = ST == 0, last = ST == F::plan.n_stages - 1;
     using Regs = typename F::template StageRegs<R>;
     Regs regs;

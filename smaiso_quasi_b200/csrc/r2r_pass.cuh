@@ -73,6 +73,13 @@ struct StoreField {
   }
 };
 
+template <class S> struct IsStoreField : std::false_type {};
+template <typename T> struct IsStoreField<StoreField<T>> : std::true_type {};
+
+template <typename T> struct Vec4;
+template <> struct Vec4<float> { using type = float4; };
+template <> struct Vec4<double> { using type = double2; };
+
 template <typename T>
 struct ScaleStore {
   Geom g;
@@ -141,14 +148,25 @@ struct GlobSnk {
   int outer, k0;
   __device__ __forceinline__ void put(int g, int n, T a, T b) const {
     const int k = k0 + 2 * g;
-    if (AXIS == 1) store_pair<T>(st, outer, n, k, a, b);
-    else store_pair<T>(st, n, outer, k, a, b);
+    if constexpr (IsStoreField<Store>::value) {
+      // plain field: (outer, n) -> element offset without 64-bit index math per pair
+      const Geom& gm = st.g;
+      const size_t row = AXIS == 1 ? size_t(outer) * gm.ny + n : size_t(n) * gm.ny + outer;
+      typename Vec2<T>::type v;
+      v.x = a;
+      v.y = b;
+      *reinterpret_cast<typename Vec2<T>::type*>(st.dst + row * gm.nz + k) = v;
+    } else if (AXIS == 1) {
+      store_pair<T>(st, outer, n, k, a, b);
+    } else {
+      store_pair<T>(st, n, outer, k, a, b);
+    }
   }
 };
 
 // Threads per CTA and the CTAs per SM the register allocation must allow.
-template <typename T> constexpr int pass_threads() { return sizeof(T) == 8 ? 128 : 256; }
-template <typename T> constexpr int pass_min_blocks() { return sizeof(T) == 8 ? 4 : 2; }
+template <typename T> constexpr int pass_threads() { return 256; }
+template <typename T> constexpr int pass_min_blocks() { return 2; }
 
 template <typename T, int N, int AXIS, int P, class Load, class Store>
 __global__ void __launch_bounds__(pass_threads<T>(), pass_min_blocks<T>()) axis_pass_kernel(Geom g, int kind, Tables<T> tb, Load ld,
@@ -298,7 +316,7 @@ __device__ __forceinline__ void tma_issue_tile(const CUtensorMap* map, T* raw, u
   }
 }
 
-template <typename T> constexpr int tma_threads() { return sizeof(T) == 8 ? 128 : 256; }
+template <typename T> constexpr int tma_threads() { return 256; }
 
 template <typename T, int N, int AXIS, int P, class Store, class Mul>
 __global__ void __launch_bounds__(tma_threads<T>(), 2)
@@ -358,12 +376,26 @@ __global__ void __launch_bounds__(tma_threads<T>(), 2)
       __syncthreads();
       issue_next();
       r2r_tile_inplace<T, N, P / 2, NT>(ex, tid, kind, work, tb);
+      // the tile's P rows lie in one x plane (P divides ny)
       const int row0 = t * P;
-      for (int e = tid; e < P * N; e += NT) {
-        const int p = e / N, n = e - p * N;
-        const int row = row0 + p;
-        const int i = row / g.ny, j = row - i * g.ny;
-        st(i, j, n, work[p * LD + n]);
+      const int i0 = row0 / g.ny, j0 = row0 - i0 * g.ny;
+      if constexpr (IsStoreField<Store>::value) {
+        constexpr int V = 16 / sizeof(T);   // 16-byte vector stores along z
+        using VT = typename Vec4<T>::type;
+        T* base = st.dst + size_t(row0) * N;
+        for (int e = tid; e < P * N / V; e += NT) {
+          const int p = (e * V) / N, n = e * V - p * N;
+          VT v;
+          T* vv = reinterpret_cast<T*>(&v);
+#pragma unroll
+          for (int u = 0; u < V; ++u) vv[u] = work[p * LD + n + u];
+          *reinterpret_cast<VT*>(base + size_t(p) * N + n) = v;
+        }
+      } else {
+        for (int e = tid; e < P * N; e += NT) {
+          const int p = e / N, n = e - p * N;
+          st(i0, j0 + p, n, work[p * LD + n]);
+        }
       }
     }
     __syncthreads();   // the next tile's first stage overwrites `work`
