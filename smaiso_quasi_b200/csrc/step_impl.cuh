@@ -207,65 +207,84 @@ template <typename T>
 __global__ void __launch_bounds__(256) project_kernel(StepCtx<T> c) {
   using A = Arith<T>;
   const Geom g = c.g;
-  const size_t sj = g.nz, si = size_t(g.ny) * g.nz;
+  const int nz = g.nz;
+  const size_t si = size_t(g.ny) * nz;
   const A scale = A(c.scale), nu = A(c.nu), inu = A(1.0 / c.nu);
-  QUASI_ROWS_BEGIN(g)
-    const A qx = A(c.vqx[i]), qy = A(c.vqy[j]), qz = A(c.vqz[k]);
-    const A sxc = c.Sx[id], syc = c.Sy[id], szc = c.Sz[id];
-    const A dvc = c.divvq[id];
-    // p^: divergence of the stress shifted back onto the cosine grid
-    {
-      const bool on = c.variant == kQuasi ? (i + j + k != 0) : (i * j * k > 0);
-      A pv = A(0);
-      if (on) {
-        const A sx = i > 0 ? A(c.Sx[id - si]) : A(0);
-        const A sy = j > 0 ? A(c.Sy[id - sj]) : A(0);
-        const A sz = k > 0 ? A(c.Sz[id - 1]) : A(0);
-        A v = -(qx * sx + qy * sy + qz * sz) * rcp(qx * qx + qy * qy + qz * qz);
-        if (c.variant == kStb) v += nu * dvc;
-        pv = scale * v;
-      }
-      c.p[id] = T(pv);
-    }
-    // v^x (i < nx-1): CM1 = scale/(nu mq), CM2 = Vs/mq  (quasi.cpp:889-899)
-    {
-      A v = A(0);
-      if (i < g.nx - 1) {
-        const A sy = j > 0 ? A(c.Sy[id + si - sj]) : A(0);
-        const A sz = k > 0 ? A(c.Sz[id + si - 1]) : A(0);
-        const A vs = A(c.vsx[i]);
-        const A inv = rcp(vs * vs + qy * qy + qz * qz);
-        const A dot = vs * sxc + qy * sy + qz * sz;
-        v = (scale * inv * inu) * (sxc - (vs * inv) * dot + nu * vs * A(c.divvq[id + si]));
-      }
-      c.vx[id] = T(v);
-    }
-    // v^y, v^z (j < ny-1, k < nz-1); Sx from the plane halo #4 delivers (quasi.cpp:1649)
-    A vy = A(0), vz = A(0);
-    if (j < g.ny - 1 && k < g.nz - 1) {
-      const int isrc = (i % c.n0 == 0) ? i - c.n0 : i - 1;
-      const size_t bx = size_t(isrc < 0 ? 0 : isrc) * si + size_t(j) * sj + k;
+  for (int row = blockIdx.x; row < g.nx * g.ny; row += gridDim.x) {
+    // everything that depends on (i, j) only
+    const int i = row / g.ny, j = row - i * g.ny;
+    const size_t base = size_t(row) * nz;
+    const A qx = A(c.vqx[i]), qy = A(c.vqy[j]);
+    const A vsx = A(c.vsx[i]), vsy = A(c.vsy[j]);
+    const bool ip = i > 0, jp = j > 0, last_x = i >= g.nx - 1, last_y = j >= g.ny - 1;
+    const bool stb = c.variant == kStb;
+    // plane "i - 1" as halo #4 delivers it to vely/velz (quasi.cpp:1649)
+    const int isrc = (i % c.n0 == 0) ? i - c.n0 : i - 1;
+    const size_t bx = size_t(isrc < 0 ? 0 : isrc) * si + size_t(j) * nz;
+    const T* Sx = c.Sx;
+    const T* Sy = c.Sy;
+    const T* Sz = c.Sz;
+    const T* Dq = c.divvq;
+    for (int k = threadIdx.x; k < nz; k += blockDim.x) {
+      const size_t id = base + k;
+      const bool kp = k > 0, klast = k >= nz - 1;
+      // every stencil value is loaded unconditionally from a clamped, in-bounds
+      // index (so all loads are in flight together) and masked afterwards
+      const size_t im = ip ? id - si : id, ipl = last_x ? id : id + si;
+      const size_t jm = jp ? id - nz : id, jpl = last_y ? id : id + nz;
+      const size_t km = kp ? id - 1 : id, kpl = klast ? id : id + 1;
+      const size_t xs = ip ? bx : base - size_t(j) * nz;   // halo source row (i > 0) or this plane's row 0
+      const A sxc = Sx[id], syc = Sy[id], szc = Sz[id], dvc = Dq[id];
+      const A sx_im = Sx[im], sy_jm = Sy[jm], sz_km = Sz[km];
+      const A sy_x = Sy[ipl - (jp ? nz : 0)], sz_x = Sz[ipl - (kp ? 1 : 0)], dq_x = Dq[ipl];
+      const A sx_y = Sx[xs + (last_y ? 0 : nz) + k], sz_y = Sz[jpl - (kp ? 1 : 0)], dq_y = Dq[jpl];
+      const A sx_z = Sx[xs + (klast ? k : k + 1)], sy_z = Sy[jm + (klast ? 0 : 1)], dq_z = Dq[kpl];
+      const A qz = A(c.vqz[k]);
+      // p^: divergence of the stress shifted back onto the cosine grid (quasi.cpp:1379-1414)
       {
-        const A sx = i > 0 ? A(c.Sx[bx + sj]) : A(0);
-        const A sz = k > 0 ? A(c.Sz[id + sj - 1]) : A(0);
-        const A vs = A(c.vsy[j]);
-        const A inv = rcp(qx * qx + vs * vs + qz * qz);
-        const A dot = qx * sx + vs * syc + qz * sz;
-        vy = (scale * inv * inu) * (syc - (vs * inv) * dot + nu * vs * A(c.divvq[id + sj]));
+        const bool on = stb ? (i * j * k > 0) : (i + j + k != 0);
+        A pv = A(0);
+        if (on) {
+          const A sx = ip ? sx_im : A(0), sy = jp ? sy_jm : A(0), sz = kp ? sz_km : A(0);
+          A v = -(qx * sx + qy * sy + qz * sz) * rcp(qx * qx + qy * qy + qz * qz);
+          if (stb) v += nu * dvc;
+          pv = scale * v;
+        }
+        c.p[id] = T(pv);
       }
+      // v^x (i < nx-1): CM1 = scale/(nu mq), CM2 = Vs/mq  (quasi.cpp:889-899, 1522-1633)
       {
-        const A sx = i > 0 ? A(c.Sx[bx + 1]) : A(0);
-        const A sy = j > 0 ? A(c.Sy[id - sj + 1]) : A(0);
-        const A vs = A(c.vsz[k]);
-        const A inv = rcp(qx * qx + qy * qy + vs * vs);
-        const A dot = qx * sx + qy * sy + vs * szc;
-        vz = (scale * inv * inu) * (szc - (vs * inv) * dot + nu * vs * A(c.divvq[id + 1]));
+        A v = A(0);
+        if (!last_x) {
+          const A sy = jp ? sy_x : A(0), sz = kp ? sz_x : A(0);
+          const A inv = rcp(vsx * vsx + qy * qy + qz * qz);
+          const A dot = vsx * sxc + qy * sy + qz * sz;
+          v = (scale * inv * inu) * (sxc - (vsx * inv) * dot + nu * vsx * dq_x);
+        }
+        c.vx[id] = T(v);
       }
+      // v^y, v^z (j < ny-1, k < nz-1)  (quasi.cpp:1683-1872)
+      A vy = A(0), vz = A(0);
+      if (!last_y && !klast) {
+        {
+          const A sx = ip ? sx_y : A(0), sz = kp ? sz_y : A(0);
+          const A inv = rcp(qx * qx + vsy * vsy + qz * qz);
+          const A dot = qx * sx + vsy * syc + qz * sz;
+          vy = (scale * inv * inu) * (syc - (vsy * inv) * dot + nu * vsy * dq_y);
+        }
+        {
+          const A vsz = A(c.vsz[k]);
+          const A sx = ip ? sx_z : A(0), sy = jp ? sy_z : A(0);
+          const A inv = rcp(qx * qx + qy * qy + vsz * vsz);
+          const A dot = qx * sx + qy * sy + vsz * szc;
+          vz = (scale * inv * inu) * (szc - (vsz * inv) * dot + nu * vsz * dq_z);
+        }
+      }
+      c.vy[id] = T(vy);
+      c.vz[id] = T(vz);
+      if (!stb) c.divv[id] = T(scale * dvc);
     }
-    c.vy[id] = T(vy);
-    c.vz[id] = T(vz);
-    if (c.variant == kQuasi) c.divv[id] = T(scale * dvc);
-  QUASI_ROWS_END
+  }
 }
 
 // Nonlinear term N (quasi.cpp:1905-1929, quasi-stb.cpp:1900-1924) -> Nq
