@@ -5,6 +5,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -35,6 +36,14 @@ class EngineBase {
 
 EngineBase* make_engine_f64(const quasi_config& cfg, std::string& err);
 EngineBase* make_engine_f32(const quasi_config& cfg, std::string& err);
+
+// QUASI_FUSED_YZ=1 selects the one-pass y+z cluster kernel (yz_plane.cuh)
+// for the plane shapes it covers; by default the y and z passes run as two
+// TMA passes, which measured faster on B200.
+inline bool fused_yz_requested() {
+  const char* v = std::getenv("QUASI_FUSED_YZ");
+  return v && v[0] == '1';
+}
 
 // Validates a configuration; returns an empty string when it is usable.
 std::string validate_config(const quasi_config& c);

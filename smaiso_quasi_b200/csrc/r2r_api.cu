@@ -22,6 +22,7 @@ struct R2RBase {
     t.err = tma_err;
     t.sms = sms;
     t.enabled = true;
+    t.yz = fused_yz_requested();
   }
 };
 
@@ -53,10 +54,8 @@ struct R2R : R2RBase {
     const Geom g{nx, ny, nz};
     cudaError_t e;
     use_tma();
-    if ((e = launch_pass<T, 2>(g, kind[2], tb.t[2], LoadField<T>{g, d}, StoreField<T>{g, d}, s)) != cudaSuccess)
-      return e;
-    if ((e = launch_pass<T, 1>(g, kind[1], tb.t[1], LoadField<T>{g, d}, StoreField<T>{g, d}, s)) != cudaSuccess)
-      return e;
+    const int k3[3] = {kind[0], kind[1], kind[2]};
+    if ((e = yz3(g, tb, k3, d, StoreField<T>{g, d}, s)) != cudaSuccess) return e;
     return launch_pass<T, 0>(g, kind[0], tb.t[0], LoadField<T>{g, d}, StoreField<T>{g, d}, s);
   }
 };

@@ -16,6 +16,7 @@
 // exact device indexing also runs (serially) in the CPU unit test.
 #pragma once
 #include <cstdint>
+#include <type_traits>
 
 #ifdef __CUDACC__
 #define QHD __host__ __device__ __forceinline__
@@ -217,11 +218,25 @@ struct SmemSnk {
   }
 };
 
-template <typename T, int N, int G, int NT>
+// Tile layouts between stages: complex element e of pencil g at
+// cb[g * GS + e * ES].  The default is pencil-major with the odd stride
+// LD = N + 1; element-major (GS = 1, ES = G) is the layout a TMA box of G
+// complex columns lands in, conflict-free for 64-bit accesses when G = 16.
+template <int N>
+struct PencilMajor {
+  static constexpr int GS = tile_ld(N), ES = 1;
+};
+template <int G>
+struct ElemMajor {
+  static constexpr int GS = 1, ES = G;
+};
+
+template <typename T, int N, int G, int NT, class L = PencilMajor<N>>
 struct TileFFT {
   static constexpr RadixPlan plan = radix_plan(N, max_radix<T>());
   static constexpr int LD = tile_ld(N);
   static_assert(plan.n_stages > 0, "unsupported transform length");
+  QHD static constexpr int at(int g, int e) { return g * L::GS + e * L::ES; }
 
   // butterflies a thread owns in a radix-R stage
   template <int R> static constexpr int per_thread() { return (G * (N / R) + NT - 1) / NT; }
@@ -271,7 +286,7 @@ struct TileFFT {
 #pragma unroll
       for (int t = 0; t < R; ++t) {
         const int e = q + s * (p + t * m);
-        r.v[c][t] = first ? first_input(src, kind, g, e, tb) : cb[g * LD + e];
+        r.v[c][t] = first ? first_input(src, kind, g, e, tb) : cb[at(g, e)];
       }
       Dft<T, R>::run(r.v[c]);
       const int step = (N / n) * p;   // W_n^{p u} = root[(N/n) p u], (N/n) p u < N
@@ -301,7 +316,7 @@ struct TileFFT {
           else { n = 2 * (N - 1 - k) + 1; if (kind == O01) sgn = T(-1); }
           snk.put(g, n, sgn * f.x, -sgn * f.y);
         } else {
-          cb[g * LD + k] = f;
+          cb[at(g, k)] = f;
         }
       }
     }
@@ -321,7 +336,7 @@ struct TileFFT {
       if (w >= G * kPairs) break;
       const int g = w % G, k = w / G;
       const int kn = (N - k) % N;
-      const Cx<T> z0 = cb[g * LD + k], z1 = cb[g * LD + kn];
+      const Cx<T> z0 = cb[at(g, k)], z1 = cb[at(g, kn)];
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const Cx<T> zk = h ? z1 : z0;
@@ -361,12 +376,22 @@ struct NoHook {
   QHD void operator()() const {}
 };
 
+// A source whose bytes ARE the tile (`kAliasesTile`): the first stage then
+// reads everything before it writes, like an in-place stage.
+template <class S, class = void> struct SrcAliasesTile {
+  static constexpr bool value = false;
+};
+template <class S> struct SrcAliasesTile<S, std::void_t<decltype(S::kAliasesTile)>> {
+  static constexpr bool value = S::kAliasesTile;
+};
+
 // `hook()` runs on every thread right after the first stage's closing barrier
 // (the moment the first stage's input is no longer needed).
-template <typename T, int N, int G, int NT, int ST, bool INPLACE, class Exec, class Src, class Snk, class Hook>
+template <typename T, int N, int G, int NT, int ST, bool INPLACE, class L, class Exec, class Src, class Snk,
+          class Hook>
 QHD void r2r_stages(Exec& ex, int tid, int kind, Cx<T>* cb, const Src& src, const Snk& snk, Tables<T> tb,
                     const Hook& hook) {
-  using F = TileFFT<T, N, G, NT>;
+  using F = TileFFT<T, N, G, NT, L>;
   if constexpr (ST < F::plan.n_stages) {
     constexpr int R = F::plan.r[ST];
     constexpr int s = stage_stride(N, ST, max_radix<T>()), n = N / s;
@@ -378,7 +403,7 @@ QHD void r2r_stages(Exec& ex, int tid, int kind, Cx<T>* cb, const Src& src, cons
     // shared buffer; otherwise only for middle stages and a forward kind's
     // last stage (both write the shared buffer they read)
     const bool global_out = last && !is_forward(kind);
-    const bool mid = INPLACE || (!first && !global_out);
+    const bool mid = INPLACE || (first ? SrcAliasesTile<Src>::value : !global_out);
     // a write half must be visible before the next read half; an inverse
     // kind's last stage writing to global memory is followed by nothing
     const bool after = !last || is_forward(kind) || INPLACE;
@@ -389,15 +414,16 @@ QHD void r2r_stages(Exec& ex, int tid, int kind, Cx<T>* cb, const Src& src, cons
       if (!after) ex.sync();   // the hook may recycle the first stage's input
       hook();
     }
-    r2r_stages<T, N, G, NT, ST + 1, INPLACE>(ex, tid, kind, cb, src, snk, tb, hook);
+    r2r_stages<T, N, G, NT, ST + 1, INPLACE, L>(ex, tid, kind, cb, src, snk, tb, hook);
   }
 }
 
-template <typename T, int N, int G, int NT, bool INPLACE, class Exec, class Src, class Snk, class Hook = NoHook>
+template <typename T, int N, int G, int NT, bool INPLACE, class L = PencilMajor<N>, class Exec, class Src, class Snk,
+          class Hook = NoHook>
 QHD void r2r_tile(Exec& ex, int tid, int kind, Cx<T>* cb, const Src& src, const Snk& snk, Tables<T> tb,
                   const Hook& hook = Hook()) {
-  using F = TileFFT<T, N, G, NT>;
-  r2r_stages<T, N, G, NT, 0, INPLACE>(ex, tid, kind, cb, src, snk, tb, hook);
+  using F = TileFFT<T, N, G, NT, L>;
+  r2r_stages<T, N, G, NT, 0, INPLACE, L>(ex, tid, kind, cb, src, snk, tb, hook);
   if (is_forward(kind)) {
     typename F::UnpackRegs regs;
     ex.phase([&](int t, typename F::UnpackRegs& rg) { F::unpack_read(t, cb, tb, rg); },

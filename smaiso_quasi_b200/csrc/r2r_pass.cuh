@@ -262,8 +262,9 @@ struct NoMul {
 
 // x / y tile source with a per-element multiplier of the OUTPUT index
 // (i, j, k): the spectral prologue of an inverse transform.
-template <typename T, int AXIS, class Mul>
+template <typename T, int AXIS, class Mul, bool ALIAS = false>
 struct MulSrc {
+  static constexpr bool kAliasesTile = ALIAS;
   const T* raw;
   int P, outer, k0;
   Mul mul;
@@ -281,6 +282,11 @@ struct MulSrc {
 };
 
 constexpr uint32_t kTmaPollLimit = 1u << 24;
+
+#ifndef QUASI_TMA_INPLACE
+#define QUASI_TMA_INPLACE 0
+#endif
+constexpr bool kTmaInPlace = QUASI_TMA_INPLACE != 0;
 
 template <int AXIS, int P>
 __device__ __forceinline__ void tile_origin(const Geom& g, int tile, int& c0, int& c1, int& c2) {
@@ -318,17 +324,27 @@ __device__ __forceinline__ void tma_issue_tile(const CUtensorMap* map, T* raw, u
 
 template <typename T> constexpr int tma_threads() { return 256; }
 
-template <typename T, int N, int AXIS, int P, class Store, class Mul>
-__global__ void __launch_bounds__(tma_threads<T>(), 2)
+// IP (x / y only): the tile is transformed in place in its raw buffer, whose
+// [n][P] layout is the element-major complex layout [n][P/2]; no padded work
+// tile, so three CTAs fit an SM.  The raw buffer is then recycled only after
+// the tile's last read.
+template <typename T, int N, int AXIS, int P, bool IP> constexpr int tma_work_elems() {
+  return IP ? 0 : ((P * tile_ld(N) + 15) / 16) * 16;
+}
+template <bool IP> constexpr int tma_min_blocks() { return IP ? 3 : 2; }
+
+template <typename T, int N, int AXIS, int P, class Store, class Mul, bool IP = false>
+__global__ void __launch_bounds__(tma_threads<T>(), tma_min_blocks<IP>())
     tma_pass_kernel(const __grid_constant__ CUtensorMap map, Geom g, int kind, Tables<T> tb, Store st, int ntiles,
                     int* err, Mul mul, int dc1, int dc2) {
+  static_assert(!IP || AXIS != 2, "in-place raw tiles are for x / y passes");
   constexpr int NT = tma_threads<T>();
   constexpr int LD = tile_ld(N);
   extern __shared__ __align__(128) unsigned char smem_raw[];
   T* raw0 = reinterpret_cast<T*>(smem_raw);
   T* raw1 = raw0 + P * N;
   T* work = raw1 + P * N;
-  uint64_t* bar = reinterpret_cast<uint64_t*>(work + ((P * LD + 15) / 16) * 16);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(work + tma_work_elems<T, N, AXIS, P, IP>());
   const int tid = threadIdx.x;
   if (tid == 0) {
     mbar_init(&bar[0], 1);
@@ -361,7 +377,17 @@ __global__ void __launch_bounds__(tma_threads<T>(), 2)
         tma_issue_tile<T, N, AXIS, P>(&map, raw, &bar[b], g, t_next, dc1, dc2);
       }
     };
-    if constexpr (AXIS != 2) {
+    if constexpr (AXIS != 2 && IP) {
+      const int kt = g.nz / P;
+      const int outer = t / kt, k0 = (t - outer * kt) * P;
+      r2r_tile<T, N, P / 2, NT, false, ElemMajor<P / 2>>(ex, tid, kind, reinterpret_cast<Cx<T>*>(raw),
+                                                          MulSrc<T, AXIS, Mul, true>{raw, P, outer, k0, mul},
+                                                          GlobSnk<T, AXIS, Store>{st, outer, k0}, tb);
+      fence_proxy_async_smem();   // this thread's writes to raw precede the copy that refills it
+      __syncthreads();            // the last read of this raw buffer is done
+      issue_next();
+      continue;
+    } else if constexpr (AXIS != 2) {
       const int kt = g.nz / P;
       const int outer = t / kt, k0 = (t - outer * kt) * P;
       r2r_tile<T, N, P / 2, NT, false>(ex, tid, kind, reinterpret_cast<Cx<T>*>(work),
@@ -402,9 +428,9 @@ __global__ void __launch_bounds__(tma_threads<T>(), 2)
   }
 }
 
-template <typename T, int N, int P>
+template <typename T, int N, int AXIS, int P, bool IP>
 inline size_t tma_smem_bytes() {
-  return size_t(2) * P * N * sizeof(T) + size_t((P * tile_ld(N) + 15) / 16) * 16 * sizeof(T) + 64;
+  return size_t(2) * P * N * sizeof(T) + size_t(tma_work_elems<T, N, AXIS, P, IP>()) * sizeof(T) + 64;
 }
 
 // Pencils per tile.  z: rows per CTA; x/y: consecutive k (coalescing width).
@@ -441,13 +467,14 @@ struct TmaConfig {
   int* err = nullptr;     // device flag, nonzero after a timed-out wait
   int sms = 148;          // CTAs per SM x SMs bounds the persistent grid
   bool enabled = true;
+  bool yz = false;        // fuse the y and z passes into one cluster pass
 };
 inline TmaConfig& tma_config() {
   static thread_local TmaConfig c;
   return c;
 }
 
-template <typename T, int N, int AXIS, int P, class Store, class Mul = NoMul>
+template <typename T, int N, int AXIS, int P, class Store, class Mul = NoMul, bool IP = kTmaInPlace && AXIS != 2>
 cudaError_t launch_tma_pass(const Geom& g, int kind, Tables<T> tb, const T* src, Store st, cudaStream_t s,
                             Mul mul = Mul(), int dc1 = 0, int dc2 = 0) {
   uint32_t box[3];
@@ -457,19 +484,21 @@ cudaError_t launch_tma_pass(const Geom& g, int kind, Tables<T> tb, const T* src,
   else { box[0] = P; box[1] = 1; box[2] = N / SUB; }
   CUtensorMap map;
   if (!MapCache::get().lookup(&map, src, int(sizeof(T)), g.nx, g.ny, g.nz, AXIS, box)) return cudaErrorNotSupported;
-  const size_t smem = tma_smem_bytes<T, N, P>();
-  auto kern = tma_pass_kernel<T, N, AXIS, P, Store, Mul>;
-  static bool configured = false;   // per instantiation
-  if (!configured) {
+  const size_t smem = tma_smem_bytes<T, N, AXIS, P, IP>();
+  auto kern = tma_pass_kernel<T, N, AXIS, P, Store, Mul, IP>;
+  static int per_sm = 0;   // per instantiation: resident CTAs per SM
+  if (per_sm == 0) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    configured = true;
+    int n = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, tma_threads<T>(), smem);
+    if (e != cudaSuccess) return e;
+    per_sm = n > 0 ? n : 1;
   }
   int tiles;
   if (AXIS == 2) tiles = (g.nx * g.ny) / P;
   else if (AXIS == 1) tiles = g.nx * (g.nz / P);
   else tiles = g.ny * (g.nz / P);
-  const int per_sm = smem * 2 <= 220 * 1024 ? 2 : 1;
   const int grid = tiles < per_sm * tma_config().sms ? tiles : per_sm * tma_config().sms;
   kern<<<grid, tma_threads<T>(), smem, s>>>(map, g, kind, tb, st, tiles, tma_config().err, mul, dc1, dc2);
   return cudaGetLastError();

@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include "r2r_pass.cuh"
+#include "yz_plane.cuh"
 
 namespace quasi {
 
@@ -136,25 +137,43 @@ template <typename T> struct StRhoq {
 // (consecutive threads -> consecutive k), computes the terms shared by its
 // outputs once, and leaves the transforms around it plain.
 // ---------------------------------------------------------------------------
-// Iterate rows (i, j) with threads over k: one 32-bit division per row.
-#define QUASI_ROWS_BEGIN(g)                                                                       \
-  for (int row = blockIdx.x; row < (g).nx * (g).ny; row += gridDim.x) {                           \
-    const int i = row / (g).ny, j = row - i * (g).ny;                                             \
-    const size_t base = size_t(row) * (g).nz;                                                     \
-    for (int k = threadIdx.x; k < (g).nz; k += blockDim.x) {                                      \
-      const size_t id = base + k;
-#define QUASI_ROWS_END \
-  }                    \
-  }
+// Elementwise stages move 16 bytes per field access: a Pack is V = 16 /
+// sizeof(T) consecutive elements of one row (nz is a multiple of 8, so packs
+// never straddle rows).  The flat stages walk packs with a grid-stride loop.
+template <typename T>
+struct alignas(16) Pack {
+  static constexpr int V = 16 / sizeof(T);
+  T v[V];
+};
+template <typename T>
+__device__ __forceinline__ Pack<T> ldp(const T* p, size_t pi) {
+  Pack<T> r;
+  *reinterpret_cast<typename Vec4<T>::type*>(r.v) = reinterpret_cast<const typename Vec4<T>::type*>(p)[pi];
+  return r;
+}
+template <typename T>
+__device__ __forceinline__ void stp(T* p, size_t pi, const Pack<T>& r) {
+  reinterpret_cast<typename Vec4<T>::type*>(p)[pi] = *reinterpret_cast<const typename Vec4<T>::type*>(r.v);
+}
+#define QUASI_PACKS(n)                                                                                   \
+  for (size_t pi = blockIdx.x * size_t(blockDim.x) + threadIdx.x; pi < (n) / Pack<T>::V;               \
+       pi += size_t(gridDim.x) * blockDim.x)
 
 // rho = kp sqrt(q0^2 psi^2 + |grad psi|^2) + rho_0   quasi.cpp:1243-1247
 template <typename T>
 __global__ void __launch_bounds__(256) rho_law_kernel(StepCtx<T> c, size_t n) {
   using A = Arith<T>;
+  constexpr int V = Pack<T>::V;
   const A kp = A(c.kp), q02 = A(c.q0 * c.q0), r0 = A(c.rho0);
-  for (size_t id = blockIdx.x * size_t(blockDim.x) + threadIdx.x; id < n; id += size_t(gridDim.x) * blockDim.x) {
-    const A ps = c.psi[id], x = c.gx[id], y = c.gy[id], z = c.gz[id];
-    c.rho[id] = T(kp * sqrt(q02 * ps * ps + x * x + y * y + z * z) + r0);
+  QUASI_PACKS(n) {
+    const Pack<T> ps = ldp(c.psi, pi), x = ldp(c.gx, pi), y = ldp(c.gy, pi), z = ldp(c.gz, pi);
+    Pack<T> r;
+#pragma unroll
+    for (int u = 0; u < V; ++u) {
+      const A p = ps.v[u], a = x.v[u], b = y.v[u], d = z.v[u];
+      r.v[u] = T(kp * sqrt(q02 * p * p + a * a + b * b + d * d) + r0);
+    }
+    stp(c.rho, pi, r);
   }
 }
 
@@ -162,16 +181,24 @@ __global__ void __launch_bounds__(256) rho_law_kernel(StepCtx<T> c, size_t n) {
 template <typename T>
 __global__ void __launch_bounds__(256) divv_kernel(StepCtx<T> c, size_t n) {
   using A = Arith<T>;
+  constexpr int V = Pack<T>::V;
   const bool on = *c.nloop > c.divv_switch;
   const A idt = A(1.0 / c.dt);
-  for (size_t id = blockIdx.x * size_t(blockDim.x) + threadIdx.x; id < n; id += size_t(gridDim.x) * blockDim.x) {
-    const A r = c.rho[id];
+  QUASI_PACKS(n) {
+    const Pack<T> r = ldp(c.rho, pi);
     if (on) {
-      const A ro = c.rho_old[id];
-      const A adv = A(c.vx[id]) * A(c.rdx[id]) + A(c.vy[id]) * A(c.rdy[id]) + A(c.vz[id]) * A(c.rdz[id]);
-      c.divv[id] = T(-((r - ro) * idt + adv) / (A(0.5) * (r + ro)));
+      const Pack<T> ro = ldp(c.rho_old, pi), vx = ldp(c.vx, pi), vy = ldp(c.vy, pi), vz = ldp(c.vz, pi);
+      const Pack<T> ax = ldp(c.rdx, pi), ay = ldp(c.rdy, pi), az = ldp(c.rdz, pi);
+      Pack<T> dv;
+#pragma unroll
+      for (int u = 0; u < V; ++u) {
+        const A rr = r.v[u], o = ro.v[u];
+        const A adv = A(vx.v[u]) * A(ax.v[u]) + A(vy.v[u]) * A(ay.v[u]) + A(vz.v[u]) * A(az.v[u]);
+        dv.v[u] = T(-((rr - o) * idt + adv) / (A(0.5) * (rr + o)));
+      }
+      stp(c.divv, pi, dv);
     }
-    c.rho_old[id] = T(r);
+    stp(c.rho_old, pi, r);
   }
 }
 
@@ -179,23 +206,36 @@ __global__ void __launch_bounds__(256) divv_kernel(StepCtx<T> c, size_t n) {
 template <typename T>
 __global__ void __launch_bounds__(256) stress_kernel(StepCtx<T> c, size_t n) {
   using A = Arith<T>;
+  constexpr int V = Pack<T>::V;
   const A beta = A(c.beta), gamma = A(c.gamma);
-  for (size_t id = blockIdx.x * size_t(blockDim.x) + threadIdx.x; id < n; id += size_t(gridDim.x) * blockDim.x) {
-    const A gx = c.gx[id], gy = c.gy[id], gz = c.gz[id];
+  QUASI_PACKS(n) {
+    const Pack<T> gx = ldp(c.gx, pi), gy = ldp(c.gy, pi), gz = ldp(c.gz, pi);
+    Pack<T> sx, sy, sz;
     if (c.variant == kQuasi) {
-      const A rho = c.rho[id];
-      const A lr = rho * A(c.lap[id]);
-      const A rd = rho * A(c.df[id]);
-      c.Sx[id] = T(lr * gx - rd * A(c.ldx[id]));
-      c.Sy[id] = T(lr * gy - rd * A(c.ldy[id]));
-      c.Sz[id] = T(lr * gz - rd * A(c.ldz[id]));
+      const Pack<T> rho = ldp(c.rho, pi), lap = ldp(c.lap, pi), df = ldp(c.df, pi);
+      const Pack<T> lx = ldp(c.ldx, pi), ly = ldp(c.ldy, pi), lz = ldp(c.ldz, pi);
+#pragma unroll
+      for (int u = 0; u < V; ++u) {
+        const A lr = A(rho.v[u]) * A(lap.v[u]);
+        const A rd = A(rho.v[u]) * A(df.v[u]);
+        sx.v[u] = T(lr * A(gx.v[u]) - rd * A(lx.v[u]));
+        sy.v[u] = T(lr * A(gy.v[u]) - rd * A(ly.v[u]));
+        sz.v[u] = T(lr * A(gz.v[u]) - rd * A(lz.v[u]));
+      }
     } else {
-      const A ps = c.psi[id];
-      const A mu = A(c.sh[id]) - beta * ps * ps * ps + gamma * ps * ps * ps * ps * ps;
-      c.Sx[id] = T(mu * gx);
-      c.Sy[id] = T(mu * gy);
-      c.Sz[id] = T(mu * gz);
+      const Pack<T> psi = ldp(c.psi, pi), sh = ldp(c.sh, pi);
+#pragma unroll
+      for (int u = 0; u < V; ++u) {
+        const A ps = psi.v[u];
+        const A mu = A(sh.v[u]) - beta * ps * ps * ps + gamma * ps * ps * ps * ps * ps;
+        sx.v[u] = T(mu * A(gx.v[u]));
+        sy.v[u] = T(mu * A(gy.v[u]));
+        sz.v[u] = T(mu * A(gz.v[u]));
+      }
     }
+    stp(c.Sx, pi, sx);
+    stp(c.Sy, pi, sy);
+    stp(c.Sz, pi, sz);
   }
 }
 
@@ -203,86 +243,147 @@ __global__ void __launch_bounds__(256) stress_kernel(StepCtx<T> c, size_t n) {
 // stress: quasi.cpp:1379-1414 (p), 1420-1872 (v), 1888-1894 (divv).  Writes
 // p^ -> p, v^ -> vx/vy/vz, scale*divv^ -> divv; the inverse transforms that
 // follow run in place on those fields.
+//
+// Blocks are (nz / V) x rows (a multiple of 32 threads): thread x owns the
+// pack k = V x .. V x + V - 1 of its row.  Every neighbour row (i +- 1,
+// j +- 1, the halo source plane) is read as whole packs; the k - 1 / k + 1
+// neighbours come from the adjacent lane's pack by a shuffle, or by one
+// scalar load at a warp edge.  Lanes whose neighbour value would cross a row
+// end are exactly the masked ones (k = 0 or k = nz - 1).
+template <typename T>
+__device__ __forceinline__ void shift_prev(const Pack<T>& a, const T* row_ptr, int k0, int lane, bool edge,
+                                           T out[Pack<T>::V]) {
+  constexpr int V = Pack<T>::V;
+  T prev = __shfl_up_sync(0xffffffffu, a.v[V - 1], 1);
+  if (edge && k0 > 0) prev = row_ptr[k0 - 1];
+  out[0] = prev;
+#pragma unroll
+  for (int u = 1; u < V; ++u) out[u] = a.v[u - 1];
+  (void)lane;
+}
+template <typename T>
+__device__ __forceinline__ void shift_next(const Pack<T>& a, const T* row_ptr, int k0, int nz, bool edge,
+                                           T out[Pack<T>::V]) {
+  constexpr int V = Pack<T>::V;
+  T next = __shfl_down_sync(0xffffffffu, a.v[0], 1);
+  if (edge && k0 + V < nz) next = row_ptr[k0 + V];
+#pragma unroll
+  for (int u = 0; u < V - 1; ++u) out[u] = a.v[u + 1];
+  out[V - 1] = next;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) project_kernel(StepCtx<T> c) {
   using A = Arith<T>;
+  constexpr int V = Pack<T>::V;
   const Geom g = c.g;
-  const int nz = g.nz;
-  const size_t si = size_t(g.ny) * nz;
+  const int nz = g.nz, nrows = g.nx * g.ny;
+  const size_t ppr = nz / V;   // packs per row
+  const int k0 = threadIdx.x * V;
+  const int lane = (threadIdx.y * blockDim.x + threadIdx.x) & 31;
+  const bool first_lane = lane == 0, last_lane = lane == 31;
   const A scale = A(c.scale), nu = A(c.nu), inu = A(1.0 / c.nu);
-  for (int row = blockIdx.x; row < g.nx * g.ny; row += gridDim.x) {
-    // everything that depends on (i, j) only
+  const bool stb = c.variant == kStb;
+  A qz[V], vsz[V];
+#pragma unroll
+  for (int u = 0; u < V; ++u) {
+    qz[u] = A(c.vqz[k0 + u]);
+    vsz[u] = A(c.vsz[k0 + u]);
+  }
+  const T* Sx = c.Sx;
+  const T* Sy = c.Sy;
+  const T* Sz = c.Sz;
+  const T* Dq = c.divvq;
+  for (int rbase = blockIdx.x * blockDim.y; rbase < nrows; rbase += gridDim.x * blockDim.y) {
+    const int row0 = rbase + threadIdx.y;
+    const bool valid = row0 < nrows;   // uniform loop: every lane reaches the shuffles
+    const int row = valid ? row0 : nrows - 1;
     const int i = row / g.ny, j = row - i * g.ny;
-    const size_t base = size_t(row) * nz;
     const A qx = A(c.vqx[i]), qy = A(c.vqy[j]);
     const A vsx = A(c.vsx[i]), vsy = A(c.vsy[j]);
     const bool ip = i > 0, jp = j > 0, last_x = i >= g.nx - 1, last_y = j >= g.ny - 1;
-    const bool stb = c.variant == kStb;
+    // neighbour rows, clamped in range (their values are masked where clamped)
+    const int r_im = ip ? row - g.ny : row;                    // (i-1, j)
+    const int r_jm = jp ? row - 1 : row;                       // (i, j-1)
+    const int r_ip = last_x ? row : row + g.ny;                // (i+1, j)
+    const int r_ipjm = r_ip - (jp ? 1 : 0);                    // (i+1, j-1)
+    const int r_jp = last_y ? row : row + 1;                   // (i, j+1)
     // plane "i - 1" as halo #4 delivers it to vely/velz (quasi.cpp:1649)
     const int isrc = (i % c.n0 == 0) ? i - c.n0 : i - 1;
-    const size_t bx = size_t(isrc < 0 ? 0 : isrc) * si + size_t(j) * nz;
-    const T* Sx = c.Sx;
-    const T* Sy = c.Sy;
-    const T* Sz = c.Sz;
-    const T* Dq = c.divvq;
-    for (int k = threadIdx.x; k < nz; k += blockDim.x) {
-      const size_t id = base + k;
+    const int r_xs = ip ? (isrc < 0 ? 0 : isrc) * g.ny + j : i * g.ny;   // halo source row, or this plane's row 0
+    const int r_xsy = r_xs + (last_y ? 0 : 1);
+    auto P = [&](const T* f, int r) { return ldp(f, size_t(r) * ppr + threadIdx.x); };
+    const Pack<T> sxc = P(Sx, row), syc = P(Sy, row), szc = P(Sz, row), dvc = P(Dq, row);
+    const Pack<T> sx_im = P(Sx, r_im), sy_jm = P(Sy, r_jm);
+    const Pack<T> sy_x = P(Sy, r_ipjm), szx = P(Sz, r_ip), dq_x = P(Dq, r_ip);
+    const Pack<T> sx_y = P(Sx, r_xsy), szy = P(Sz, r_jp), dq_y = P(Dq, r_jp);
+    const Pack<T> sxs = P(Sx, r_xs);
+    // k - 1 neighbours: Sz(i,j), Sz(i+1,j), Sz(i,j+1); k + 1: Sx(src,j), Sy(i,j-1), Dq(i,j)
+    T sz_km[V], sz_x[V], sz_y[V], sx_z[V], sy_z[V], dq_z[V];
+    shift_prev(szc, Sz + size_t(row) * nz, k0, lane, first_lane, sz_km);
+    shift_prev(szx, Sz + size_t(r_ip) * nz, k0, lane, first_lane, sz_x);
+    shift_prev(szy, Sz + size_t(r_jp) * nz, k0, lane, first_lane, sz_y);
+    shift_next(sxs, Sx + size_t(r_xs) * nz, k0, nz, last_lane, sx_z);
+    shift_next(sy_jm, Sy + size_t(r_jm) * nz, k0, nz, last_lane, sy_z);
+    shift_next(dvc, Dq + size_t(row) * nz, k0, nz, last_lane, dq_z);
+    Pack<T> op, ovx, ovy, ovz, odv;
+#pragma unroll
+    for (int u = 0; u < V; ++u) {
+      const int k = k0 + u;
       const bool kp = k > 0, klast = k >= nz - 1;
-      // every stencil value is loaded unconditionally from a clamped, in-bounds
-      // index (so all loads are in flight together) and masked afterwards
-      const size_t im = ip ? id - si : id, ipl = last_x ? id : id + si;
-      const size_t jm = jp ? id - nz : id, jpl = last_y ? id : id + nz;
-      const size_t km = kp ? id - 1 : id, kpl = klast ? id : id + 1;
-      const size_t xs = ip ? bx : base - size_t(j) * nz;   // halo source row (i > 0) or this plane's row 0
-      const A sxc = Sx[id], syc = Sy[id], szc = Sz[id], dvc = Dq[id];
-      const A sx_im = Sx[im], sy_jm = Sy[jm], sz_km = Sz[km];
-      const A sy_x = Sy[ipl - (jp ? nz : 0)], sz_x = Sz[ipl - (kp ? 1 : 0)], dq_x = Dq[ipl];
-      const A sx_y = Sx[xs + (last_y ? 0 : nz) + k], sz_y = Sz[jpl - (kp ? 1 : 0)], dq_y = Dq[jpl];
-      const A sx_z = Sx[xs + (klast ? k : k + 1)], sy_z = Sy[jm + (klast ? 0 : 1)], dq_z = Dq[kpl];
-      const A qz = A(c.vqz[k]);
       // p^: divergence of the stress shifted back onto the cosine grid (quasi.cpp:1379-1414)
       {
         const bool on = stb ? (i * j * k > 0) : (i + j + k != 0);
         A pv = A(0);
         if (on) {
-          const A sx = ip ? sx_im : A(0), sy = jp ? sy_jm : A(0), sz = kp ? sz_km : A(0);
-          A v = -(qx * sx + qy * sy + qz * sz) * rcp(qx * qx + qy * qy + qz * qz);
-          if (stb) v += nu * dvc;
+          const A sx = ip ? A(sx_im.v[u]) : A(0), sy = jp ? A(sy_jm.v[u]) : A(0), sz = kp ? A(sz_km[u]) : A(0);
+          A v = -(qx * sx + qy * sy + qz[u] * sz) * rcp(qx * qx + qy * qy + qz[u] * qz[u]);
+          if (stb) v += nu * A(dvc.v[u]);
           pv = scale * v;
         }
-        c.p[id] = T(pv);
+        op.v[u] = T(pv);
       }
       // v^x (i < nx-1): CM1 = scale/(nu mq), CM2 = Vs/mq  (quasi.cpp:889-899, 1522-1633)
       {
         A v = A(0);
         if (!last_x) {
-          const A sy = jp ? sy_x : A(0), sz = kp ? sz_x : A(0);
-          const A inv = rcp(vsx * vsx + qy * qy + qz * qz);
-          const A dot = vsx * sxc + qy * sy + qz * sz;
-          v = (scale * inv * inu) * (sxc - (vsx * inv) * dot + nu * vsx * dq_x);
+          const A s0 = sxc.v[u];
+          const A sy = jp ? A(sy_x.v[u]) : A(0), sz = kp ? A(sz_x[u]) : A(0);
+          const A inv = rcp(vsx * vsx + qy * qy + qz[u] * qz[u]);
+          const A dot = vsx * s0 + qy * sy + qz[u] * sz;
+          v = (scale * inv * inu) * (s0 - (vsx * inv) * dot + nu * vsx * A(dq_x.v[u]));
         }
-        c.vx[id] = T(v);
+        ovx.v[u] = T(v);
       }
       // v^y, v^z (j < ny-1, k < nz-1)  (quasi.cpp:1683-1872)
       A vy = A(0), vz = A(0);
       if (!last_y && !klast) {
         {
-          const A sx = ip ? sx_y : A(0), sz = kp ? sz_y : A(0);
-          const A inv = rcp(qx * qx + vsy * vsy + qz * qz);
-          const A dot = qx * sx + vsy * syc + qz * sz;
-          vy = (scale * inv * inu) * (syc - (vsy * inv) * dot + nu * vsy * dq_y);
+          const A s0 = syc.v[u];
+          const A sx = ip ? A(sx_y.v[u]) : A(0), sz = kp ? A(sz_y[u]) : A(0);
+          const A inv = rcp(qx * qx + vsy * vsy + qz[u] * qz[u]);
+          const A dot = qx * sx + vsy * s0 + qz[u] * sz;
+          vy = (scale * inv * inu) * (s0 - (vsy * inv) * dot + nu * vsy * A(dq_y.v[u]));
         }
         {
-          const A vsz = A(c.vsz[k]);
-          const A sx = ip ? sx_z : A(0), sy = jp ? sy_z : A(0);
-          const A inv = rcp(qx * qx + qy * qy + vsz * vsz);
-          const A dot = qx * sx + qy * sy + vsz * szc;
-          vz = (scale * inv * inu) * (szc - (vsz * inv) * dot + nu * vsz * dq_z);
+          const A s0 = szc.v[u];
+          const A sx = ip ? A(sx_z[u]) : A(0), sy = jp ? A(sy_z[u]) : A(0);
+          const A inv = rcp(qx * qx + qy * qy + vsz[u] * vsz[u]);
+          const A dot = qx * sx + qy * sy + vsz[u] * s0;
+          vz = (scale * inv * inu) * (s0 - (vsz[u] * inv) * dot + nu * vsz[u] * A(dq_z[u]));
         }
       }
-      c.vy[id] = T(vy);
-      c.vz[id] = T(vz);
-      if (!stb) c.divv[id] = T(scale * dvc);
+      ovy.v[u] = T(vy);
+      ovz.v[u] = T(vz);
+      odv.v[u] = T(scale * A(dvc.v[u]));
+    }
+    if (valid) {
+      const size_t pi = size_t(row) * ppr + threadIdx.x;
+      stp(c.p, pi, op);
+      stp(c.vx, pi, ovx);
+      stp(c.vy, pi, ovy);
+      stp(c.vz, pi, ovz);
+      if (!stb) stp(c.divv, pi, odv);
     }
   }
 }
@@ -291,53 +392,92 @@ __global__ void __launch_bounds__(256) project_kernel(StepCtx<T> c) {
 template <typename T>
 __global__ void __launch_bounds__(256) nonlinear_kernel(StepCtx<T> c, size_t n) {
   using A = Arith<T>;
+  constexpr int V = Pack<T>::V;
   const bool pcoup = *c.nloop > c.divv_switch + 1;
   const A ep = A(c.ep), beta = A(c.beta), gamma = A(c.gamma), cp = A(c.kp / (c.rho_s * c.rho_s));
-  for (size_t id = blockIdx.x * size_t(blockDim.x) + threadIdx.x; id < n; id += size_t(gridDim.x) * blockDim.x) {
-    const A ps = c.psi[id];
-    const A p3 = ps * ps * ps, p5 = p3 * ps * ps;
-    const A adv = A(c.vx[id]) * A(c.gx[id]) + A(c.vy[id]) * A(c.gy[id]) + A(c.vz[id]) * A(c.gz[id]);
-    A nv;
+  QUASI_PACKS(n) {
+    const Pack<T> psi = ldp(c.psi, pi);
+    const Pack<T> vx = ldp(c.vx, pi), vy = ldp(c.vy, pi), vz = ldp(c.vz, pi);
+    const Pack<T> gx = ldp(c.gx, pi), gy = ldp(c.gy, pi), gz = ldp(c.gz, pi);
+    A adv[V], p3[V], p5[V];
+#pragma unroll
+    for (int u = 0; u < V; ++u) {
+      const A ps = psi.v[u];
+      p3[u] = ps * ps * ps;
+      p5[u] = p3[u] * ps * ps;
+      adv[u] = A(vx.v[u]) * A(gx.v[u]) + A(vy.v[u]) * A(gy.v[u]) + A(vz.v[u]) * A(gz.v[u]);
+    }
+    Pack<T> out;
     if (c.variant == kQuasi) {
-      const A rho = c.rho[id];
-      nv = rho * (ep * ps - A(c.df[id]) + beta * p3 - gamma * p5) - rho * A(c.lap[id]) - adv;
+      const Pack<T> rho = ldp(c.rho, pi), df = ldp(c.df, pi), lap = ldp(c.lap, pi);
+#pragma unroll
+      for (int u = 0; u < V; ++u) {
+        const A r = rho.v[u], ps = psi.v[u];
+        out.v[u] = T(r * (ep * ps - A(df.v[u]) + beta * p3[u] - gamma * p5[u]) - r * A(lap.v[u]) - adv[u]);
+      }
       if (pcoup) {
-        const A a = c.rdx[id], b = c.rdy[id], d = c.rdz[id];
-        nv += A(c.p[id]) * cp * sqrt(a * a + b * b + d * d);
+        const Pack<T> a = ldp(c.rdx, pi), b = ldp(c.rdy, pi), d = ldp(c.rdz, pi), p = ldp(c.p, pi);
+#pragma unroll
+        for (int u = 0; u < V; ++u) {
+          const A x = a.v[u], y = b.v[u], z = d.v[u];
+          out.v[u] = T(A(out.v[u]) + A(p.v[u]) * cp * sqrt(x * x + y * y + z * z));
+        }
       }
     } else {
       if (c.store_dtpsi) {
-        const A mu = A(c.sh[id]) - beta * p3 + gamma * p5;
-        c.dtpsi[id] = T(-mu - adv);   // quasi-stb.cpp:1909-1912, rho == 1
+        const Pack<T> sh = ldp(c.sh, pi);
+        Pack<T> dt;
+#pragma unroll
+        for (int u = 0; u < V; ++u) dt.v[u] = T(-(A(sh.v[u]) - beta * p3[u] + gamma * p5[u]) - adv[u]);   // quasi-stb.cpp:1909-1912, rho == 1
+        stp(c.dtpsi, pi, dt);
       }
-      nv = beta * p3 - gamma * p5 - adv;
+#pragma unroll
+      for (int u = 0; u < V; ++u) out.v[u] = T(beta * p3[u] - gamma * p5[u] - adv[u]);
     }
-    c.Nq[id] = T(nv);
+    stp(c.Nq, pi, out);
   }
 }
 
-// Semi-implicit update -> psiq_new (quasi.cpp:1944-1962, quasi-stb.cpp:1946-1958)
+// Semi-implicit update -> psiq_new (quasi.cpp:1944-1962, quasi-stb.cpp:1946-1958).
+// Blocks are (nz / V) x rows: thread x owns the pack at k = V x of row
+// blockIdx.x * blockDim.y + y (then + gridDim.x * blockDim.y ...).
 template <typename T>
 __global__ void __launch_bounds__(256) update_kernel(StepCtx<T> c) {
+  constexpr int V = Pack<T>::V;
   const Geom g = c.g;
   const bool first = *c.nloop == 1;
-  const double dtd2 = c.dt / 2;
-  QUASI_ROWS_BEGIN(g)
-    const double q2 = mq2c(c, i, j, k);
-    const double alin = c.ep - c.alpha * sq(c.q0 * c.q0 - q2);
-    const double pq = c.psiq[id];
-    const double nq = c.Nq[id];
-    const double nq_old = first ? nq : double(c.Nq_old[id]);   // :1936-1938
-    double nv;
-    if (c.variant == kQuasi) {
-      const double c1 = 2.0 - c.dt * c.rho_m * alin, c2 = 1.5 - c.dt * c.rho_m * alin;   // :886-887
-      nv = (c1 * pq - 0.5 * double(c.psiq_old[id]) + dtd2 * c.scale * (3.0 * nq - nq_old)) / c2;
-    } else {
-      const double c1 = 1.0 + dtd2 * alin, c2 = 1.0 - dtd2 * alin;   // quasi-stb.cpp:855-856
-      nv = (c1 * pq + dtd2 * c.scale * (3.0 * nq - nq_old)) / c2;
+  const double dtd2 = c.dt / 2, dsc = dtd2 * c.scale;
+  const int k0 = threadIdx.x * V;
+  double qz2[V];
+#pragma unroll
+  for (int u = 0; u < V; ++u) qz2[u] = sq(c.vqz[k0 + u]);
+  const size_t ppr = g.nz / V;   // packs per row
+  for (int row = blockIdx.x * blockDim.y + threadIdx.y; row < g.nx * g.ny; row += gridDim.x * blockDim.y) {
+    const int i = row / g.ny, j = row - i * g.ny;
+    const double qxy = sq(c.vqx[i]) + sq(c.vqy[j]);
+    const size_t pi = size_t(row) * ppr + threadIdx.x;
+    const Pack<T> pq = ldp(c.psiq, pi), nq = ldp(c.Nq, pi);
+    const Pack<T> nqo = first ? nq : ldp(c.Nq_old, pi);   // :1936-1938
+    Pack<T> pqo;
+    if (c.variant == kQuasi) pqo = ldp(c.psiq_old, pi);
+    Pack<T> out;
+#pragma unroll
+    for (int u = 0; u < V; ++u) {
+      const double q2 = qxy + qz2[u];
+      const double alin = c.ep - c.alpha * sq(c.q0 * c.q0 - q2);
+      const double forcing = dsc * (3.0 * double(nq.v[u]) - double(nqo.v[u]));
+      double nv;
+      if (c.variant == kQuasi) {
+        const double c1 = 2.0 - c.dt * c.rho_m * alin, c2 = 1.5 - c.dt * c.rho_m * alin;   // :886-887
+        nv = (c1 * double(pq.v[u]) - 0.5 * double(pqo.v[u]) + forcing) / c2;
+      } else {
+        const double c1 = 1.0 + dtd2 * alin, c2 = 1.0 - dtd2 * alin;   // quasi-stb.cpp:855-856
+        nv = (c1 * double(pq.v[u]) + forcing) / c2;
+      }
+      out.v[u] = T(nv);
     }
-    c.psiq_new[id] = T(nv);
-  QUASI_ROWS_END
+    stp(c.psiq_new, pi, out);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -348,15 +488,27 @@ struct AxisTables {
   Tables<T> t[3];
 };
 
-// Inverse: x pass (loader -> dst), y pass, z pass (storer).
+// y and z passes of `src` (plain field) into `st`: one cluster pass when the
+// plane shape allows it, else two passes (the second in place on st.dst).
+template <typename T, class Store>
+cudaError_t yz3(const Geom& g, const AxisTables<T>& tb, const int kinds[3], T* src, Store st, cudaStream_t s) {
+  if constexpr (IsStoreField<Store>::value) {
+    cudaError_t e = launch_yz<T>(g, kinds[1], kinds[2], tb.t[1], tb.t[2], src, st.dst, s);
+    if (e != cudaErrorNotSupported) return e;
+  }
+  cudaError_t e;
+  if ((e = launch_pass<T, 1>(g, kinds[1], tb.t[1], LoadField<T>{g, src}, StoreField<T>{g, src}, s)) != cudaSuccess)
+    return e;
+  return launch_pass<T, 2>(g, kinds[2], tb.t[2], LoadField<T>{g, src}, st, s);
+}
+
+// Inverse: x pass (loader -> dst), then y and z (storer).
 template <typename T, class Load, class Store>
 cudaError_t inverse3(const Geom& g, const AxisTables<T>& tb, const int kinds[3], Load ld, T* dst, Store st,
                      cudaStream_t s) {
   cudaError_t e;
   if ((e = launch_pass<T, 0>(g, kinds[0], tb.t[0], ld, StoreField<T>{g, dst}, s)) != cudaSuccess) return e;
-  if ((e = launch_pass<T, 1>(g, kinds[1], tb.t[1], LoadField<T>{g, dst}, StoreField<T>{g, dst}, s)) != cudaSuccess)
-    return e;
-  return launch_pass<T, 2>(g, kinds[2], tb.t[2], LoadField<T>{g, dst}, st, s);
+  return yz3(g, tb, kinds, dst, st, s);
 }
 
 // Inverse with a spectral multiplier: x pass on mul * src[shifted] -> dst
@@ -366,19 +518,28 @@ cudaError_t inverse3_mul(const Geom& g, const AxisTables<T>& tb, const int kinds
                          int dj, StX stx, T* dst, cudaStream_t s) {
   cudaError_t e;
   if ((e = launch_mul_x_pass<T>(g, kinds[0], tb.t[0], src, mul, di, dj, stx, s)) != cudaSuccess) return e;
-  if ((e = launch_pass<T, 1>(g, kinds[1], tb.t[1], LoadField<T>{g, dst}, StoreField<T>{g, dst}, s)) != cudaSuccess)
-    return e;
-  return launch_pass<T, 2>(g, kinds[2], tb.t[2], LoadField<T>{g, dst}, StoreField<T>{g, dst}, s);
+  return yz3(g, tb, kinds, dst, StoreField<T>{g, dst}, s);
 }
 
-// Forward: z pass (loader -> dst), y pass, x pass (storer).
+// Forward: z and y (loader -> dst), then x pass (storer).  A plain field
+// loader takes the fused cluster pass.
 template <typename T, class Load, class Store>
 cudaError_t forward3(const Geom& g, const AxisTables<T>& tb, const int kinds[3], Load ld, T* dst, Store st,
                      cudaStream_t s) {
   cudaError_t e;
-  if ((e = launch_pass<T, 2>(g, kinds[2], tb.t[2], ld, StoreField<T>{g, dst}, s)) != cudaSuccess) return e;
-  if ((e = launch_pass<T, 1>(g, kinds[1], tb.t[1], LoadField<T>{g, dst}, StoreField<T>{g, dst}, s)) != cudaSuccess)
-    return e;
+  bool fused = false;
+  if constexpr (std::is_same<Load, LoadField<T>>::value) {
+    e = launch_yz<T>(g, kinds[1], kinds[2], tb.t[1], tb.t[2], ld.src, dst, s);
+    if (e != cudaErrorNotSupported) {
+      if (e != cudaSuccess) return e;
+      fused = true;
+    }
+  }
+  if (!fused) {
+    if ((e = launch_pass<T, 2>(g, kinds[2], tb.t[2], ld, StoreField<T>{g, dst}, s)) != cudaSuccess) return e;
+    if ((e = launch_pass<T, 1>(g, kinds[1], tb.t[1], LoadField<T>{g, dst}, StoreField<T>{g, dst}, s)) != cudaSuccess)
+      return e;
+  }
   return launch_pass<T, 0>(g, kinds[0], tb.t[0], LoadField<T>{g, dst}, st, s);
 }
 
@@ -400,7 +561,26 @@ static __global__ void bump_counter_kernel(int* n) { *n += 1; }
     if (e_ != cudaSuccess) return e_;         \
   } while (0)
 
-constexpr int kEwBlocks = 148 * 8;   // elementwise grid: 8 x 256 threads per SM
+// Persistent elementwise grids: the blocks of `kern` resident per SM (from
+// its occupancy at `threads` per block) times the SMs, so every block is
+// running from the start and the grid-stride loops end together.
+template <class K>
+inline int ew_grid(K kern, int threads) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, 0) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  return per_sm * tma_config().sms;
+}
+// Row-pack blocks: nz / V threads per row times the most rows that keep the
+// block within 256 threads and a whole number of warps.
+template <typename T>
+inline dim3 row_block(int nz) {
+  const int tx = nz / Pack<T>::V;
+  int ty = tx >= 256 ? 1 : 256 / tx;
+  while (ty > 1 && (tx * ty) % 32) --ty;
+  return dim3(tx, ty);
+}
+#define QUASI_EW(kern, ...) kern<<<ew_grid(kern, 256), 256, 0, s>>>(__VA_ARGS__)
 
 // One time step, enqueued on `s` (captured into a CUDA graph by the caller).
 template <typename T>
@@ -426,12 +606,12 @@ cudaError_t enqueue_step(const StepCtx<T>& c, const AxisTables<T>& tb, int* nloo
     QUASI_TRY(inverse3_mul(g, tb, kiSTy, c.psiq, MGrad<T, 1, true>{c}, 0, 1, st(c.ldy), c.ldy, s));
     QUASI_TRY(inverse3_mul(g, tb, kiSTz, c.psiq, MGrad<T, 2, true>{c}, 0, 0, StShiftK<T>{g, c.ldz}, c.ldz, s));
     // a5 density + filter quasi.cpp:1237-1268 (rho doubles as the scratch)
-    rho_law_kernel<T><<<kEwBlocks, 256, 0, s>>>(c, n);
+    QUASI_EW(rho_law_kernel<T>, c, n);
     QUASI_TRY(cudaGetLastError());
     QUASI_TRY(forward3(g, tb, kCT, ld(c.rho), c.rho, StRhoq<T>{c}, s));
     QUASI_TRY(inverse3(g, tb, kiCT, ld(c.rhoq), c.rho, st(c.rho), s));
     // a6 divv quasi.cpp:1273-1293
-    divv_kernel<T><<<kEwBlocks, 256, 0, s>>>(c, n);
+    QUASI_EW(divv_kernel<T>, c, n);
     QUASI_TRY(cudaGetLastError());
     QUASI_TRY(forward3(g, tb, kCT, ld(c.divv), c.divvq, st(c.divvq), s));
   } else {
@@ -443,13 +623,20 @@ cudaError_t enqueue_step(const StepCtx<T>& c, const AxisTables<T>& tb, int* nloo
     // rho == 1, divv == 0, grad rho == 0 (rhoq never leaves 0): quasi-stb.cpp:1232
   }
   // a7 stress quasi.cpp:1298-1330
-  stress_kernel<T><<<kEwBlocks, 256, 0, s>>>(c, n);
+  QUASI_EW(stress_kernel<T>, c, n);
   QUASI_TRY(cudaGetLastError());
   QUASI_TRY(forward3(g, tb, kSTx, ld(c.Sx), c.Sx, st(c.Sx), s));
   QUASI_TRY(forward3(g, tb, kSTy, ld(c.Sy), c.Sy, st(c.Sy), s));
   QUASI_TRY(forward3(g, tb, kSTz, ld(c.Sz), c.Sz, st(c.Sz), s));
   // a8 pressure, a9 velocity, a10 scaled divv quasi.cpp:1336-1900
-  project_kernel<T><<<kEwBlocks, 256, 0, s>>>(c);
+  {
+    const dim3 blk = row_block<T>(g.nz);
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, project_kernel<T>, blk.x * blk.y, 0) != cudaSuccess ||
+        per_sm < 1)
+      per_sm = 1;
+    project_kernel<T><<<per_sm * tma_config().sms, blk, 0, s>>>(c);
+  }
   QUASI_TRY(cudaGetLastError());
   if (c.variant == kQuasi) QUASI_TRY(inverse3(g, tb, kiCT, ld(c.p), c.p, st(c.p), s));
   QUASI_TRY(inverse3(g, tb, kiSTx, ld(c.vx), c.vx, st(c.vx), s));
@@ -457,11 +644,18 @@ cudaError_t enqueue_step(const StepCtx<T>& c, const AxisTables<T>& tb, int* nloo
   QUASI_TRY(inverse3(g, tb, kiSTz, ld(c.vz), c.vz, st(c.vz), s));
   if (c.variant == kQuasi) QUASI_TRY(inverse3(g, tb, kiCT, ld(c.divv), c.divv, st(c.divv), s));
   // a11 nonlinear term quasi.cpp:1905-1939
-  nonlinear_kernel<T><<<kEwBlocks, 256, 0, s>>>(c, n);
+  QUASI_EW(nonlinear_kernel<T>, c, n);
   QUASI_TRY(cudaGetLastError());
   QUASI_TRY(forward3(g, tb, kCT, ld(c.Nq), c.Nq, st(c.Nq), s));
   // a12 update + iCT quasi.cpp:1944-1965
-  update_kernel<T><<<kEwBlocks, 256, 0, s>>>(c);
+  {
+    const dim3 blk = row_block<T>(g.nz);
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, update_kernel<T>, blk.x * blk.y, 0) != cudaSuccess ||
+        per_sm < 1)
+      per_sm = 1;
+    update_kernel<T><<<per_sm * tma_config().sms, blk, 0, s>>>(c);
+  }
   QUASI_TRY(cudaGetLastError());
   QUASI_TRY(inverse3(g, tb, kiCT, ld(c.psiq_new), c.tmp, st(c.psi_new), s));   // psi_old <- psi by rotation
   return cudaSuccess;
