@@ -115,8 +115,11 @@ class Engine : public EngineBase {
       for (int i = 0; i < n; ++i) h.push_back(1.0 * M_PI * i / (d * n));
       for (int i = 0; i < n; ++i) h.push_back(1.0 * M_PI * (i + 1) / (d * n));
     }
-    if (!cuda_ok(cudaMalloc(&tabs_, h.size() * sizeof(double)), "malloc")) return QUASI_ERR_CUDA;
-    if (!cuda_ok(cudaMemcpy(tabs_, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice), "memcpy"))
+    // doubles, then the same values in the storage type
+    std::vector<T> ht(h.begin(), h.end());
+    if (!cuda_ok(cudaMalloc(&tabs_, h.size() * (sizeof(double) + sizeof(T))), "malloc")) return QUASI_ERR_CUDA;
+    if (!cuda_ok(cudaMemcpy(tabs_, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice), "memcpy") ||
+        !cuda_ok(cudaMemcpy(tabs_ + h.size(), ht.data(), ht.size() * sizeof(T), cudaMemcpyHostToDevice), "memcpy"))
       return QUASI_ERR_CUDA;
     for (int a = 0; a < 3; ++a)
       if (!cuda_ok(tw_[a].upload(len[a]), "twiddles")) return QUASI_ERR_CUDA;
@@ -273,6 +276,8 @@ class Engine : public EngineBase {
     auto one = [&]() -> cudaError_t {
       if (axis == 0) return launch_pass<T, 0>(g_, E01, tb_.t[0], LoadField<T>{g_, d}, StoreField<T>{g_, d}, stream_);
       if (axis == 1) return launch_pass<T, 1>(g_, E01, tb_.t[1], LoadField<T>{g_, d}, StoreField<T>{g_, d}, stream_);
+      const cudaError_t e = launch_zpass<T>(g_, E01, tb_.t[2], d, d, stream_);
+      if (e != cudaErrorNotSupported) return e;
       return launch_pass<T, 2>(g_, E01, tb_.t[2], LoadField<T>{g_, d}, StoreField<T>{g_, d}, stream_);
     };
     if (!cuda_ok(one(), "pass")) return QUASI_ERR_CUDA;   // warm
@@ -354,7 +359,7 @@ class Engine : public EngineBase {
     return false;
   }
 
-  void build_ctx(const std::vector<double>&) {
+  void build_ctx(const std::vector<double>& h) {
     T* f = static_cast<T*>(slab_);
     auto next = [&]() { T* p = f; f += n_; return p; };
     c_.g = g_;
@@ -362,6 +367,10 @@ class Engine : public EngineBase {
     c_.vqx = t;                 c_.vsx = t + g_.nx;
     c_.vqy = t + 2 * g_.nx;     c_.vsy = c_.vqy + g_.ny;
     c_.vqz = t + 2 * g_.nx + 2 * g_.ny; c_.vsz = c_.vqz + g_.nz;
+    const T* tt = reinterpret_cast<const T*>(tabs_ + h.size());
+    c_.tqx = tt;                 c_.tsx = tt + g_.nx;
+    c_.tqy = tt + 2 * g_.nx;     c_.tsy = c_.tqy + g_.ny;
+    c_.tqz = tt + 2 * g_.nx + 2 * g_.ny; c_.tsz = c_.tqz + g_.nz;
     const bool quasi = cfg_.variant == QUASI_VARIANT_QUASI;
     c_.ep = -0.001 * cfg_.ep_arg;                                   // quasi.cpp:187
     c_.alpha = cfg_.alpha; c_.beta = cfg_.beta; c_.gamma = cfg_.gamma; c_.q0 = cfg_.q0;

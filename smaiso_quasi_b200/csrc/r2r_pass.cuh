@@ -275,8 +275,8 @@ struct MulSrc {
     if constexpr (Mul::kActive) {
       const int k = k0 + 2 * g;
       const int i = AXIS == 1 ? outer : n, j = AXIS == 1 ? n : outer;
-      a = T(double(a) * mul(i, j, k));
-      b = T(double(b) * mul(i, j, k + 1));
+      a = a * mul(i, j, k);
+      b = b * mul(i, j, k + 1);
     }
   }
 };
@@ -336,7 +336,7 @@ template <bool IP> constexpr int tma_min_blocks() { return IP ? 3 : 2; }
 template <typename T, int N, int AXIS, int P, class Store, class Mul, bool IP = false>
 __global__ void __launch_bounds__(tma_threads<T>(), tma_min_blocks<IP>())
     tma_pass_kernel(const __grid_constant__ CUtensorMap map, Geom g, int kind, Tables<T> tb, Store st, int ntiles,
-                    int* err, Mul mul, int dc1, int dc2) {
+                    int* err, Mul mul, int dc1, int dc2, int ks) {
   static_assert(!IP || AXIS != 2, "in-place raw tiles are for x / y passes");
   constexpr int NT = tma_threads<T>();
   constexpr int LD = tile_ld(N);
@@ -394,10 +394,18 @@ __global__ void __launch_bounds__(tma_threads<T>(), tma_min_blocks<IP>())
                                         MulSrc<T, AXIS, Mul>{raw, P, outer, k0, mul},
                                         GlobSnk<T, AXIS, Store>{st, outer, k0}, tb, issue_next);
     } else {
-      // dense rows -> padded in-place tile (both sides contiguous in n)
-      for (int e = tid; e < P * N; e += NT) {
-        const int p = e / N, n = e - p * N;
-        work[p * LD + n] = raw[e];
+      // dense rows -> padded in-place tile (both sides contiguous in n); ks = 1
+      // stages row[n + 1] at n and zero at the top
+      if (ks == 0) {
+        for (int e = tid; e < P * N; e += NT) {
+          const int p = e / N, n = e - p * N;
+          work[p * LD + n] = raw[e];
+        }
+      } else {
+        for (int e = tid; e < P * N; e += NT) {
+          const int p = e / N, n = e - p * N;
+          work[p * LD + n] = n + 1 < N ? raw[e + 1] : T(0);
+        }
       }
       __syncthreads();
       issue_next();
@@ -476,7 +484,7 @@ inline TmaConfig& tma_config() {
 
 template <typename T, int N, int AXIS, int P, class Store, class Mul = NoMul, bool IP = kTmaInPlace && AXIS != 2>
 cudaError_t launch_tma_pass(const Geom& g, int kind, Tables<T> tb, const T* src, Store st, cudaStream_t s,
-                            Mul mul = Mul(), int dc1 = 0, int dc2 = 0) {
+                            Mul mul = Mul(), int dc1 = 0, int dc2 = 0, int ks = 0) {
   uint32_t box[3];
   constexpr int SUB = (N + 255) / 256;
   if (AXIS == 2) { box[0] = N; box[1] = P; box[2] = 1; }
@@ -500,7 +508,7 @@ cudaError_t launch_tma_pass(const Geom& g, int kind, Tables<T> tb, const T* src,
   else if (AXIS == 1) tiles = g.nx * (g.nz / P);
   else tiles = g.ny * (g.nz / P);
   const int grid = tiles < per_sm * tma_config().sms ? tiles : per_sm * tma_config().sms;
-  kern<<<grid, tma_threads<T>(), smem, s>>>(map, g, kind, tb, st, tiles, tma_config().err, mul, dc1, dc2);
+  kern<<<grid, tma_threads<T>(), smem, s>>>(map, g, kind, tb, st, tiles, tma_config().err, mul, dc1, dc2, ks);
   return cudaGetLastError();
 }
 
@@ -532,10 +540,19 @@ cudaError_t launch_pass(const Geom& g, int kind, Tables<T> tb, Load ld, Store st
 #undef QUASI_PASS_CASE
 }
 
+// z loads shifted by one along k: row[k + 1], zero at the top.
+template <typename T>
+struct ShiftKLoad {
+  Geom g;
+  const T* src;
+  __device__ T operator()(int i, int j, int k) const { return k + 1 < g.nz ? src[lin(g, i, j, k + 1)] : T(0); }
+};
+
 // Plain field loads: the persistent TMA kernel when the tile fits a box,
-// otherwise the general kernel above.
+// otherwise the general kernel above.  ks = 1 (z passes only) loads row[k + 1].
 template <typename T, int AXIS, class Store>
-cudaError_t launch_pass(const Geom& g, int kind, Tables<T> tb, LoadField<T> ld, Store st, cudaStream_t s) {
+cudaError_t launch_pass(const Geom& g, int kind, Tables<T> tb, LoadField<T> ld, Store st, cudaStream_t s,
+                        int ks = 0) {
   const int n = AXIS == 0 ? g.nx : (AXIS == 1 ? g.ny : g.nz);
   const long extent = AXIS == 2 ? long(g.nx) * g.ny : long(g.nz);
   if (tma_config().enabled && tma_config().err) {
@@ -543,7 +560,7 @@ cudaError_t launch_pass(const Geom& g, int kind, Tables<T> tb, LoadField<T> ld, 
     case NN: {                                                                                         \
       constexpr int P = pass_pencils<T>(NN);                                                           \
       const bool fits = extent % P == 0 && (AXIS != 2 || (NN <= 256 && g.ny % P == 0));                \
-      if (fits) return launch_tma_pass<T, NN, AXIS, P>(g, kind, tb, ld.src, st, s);                    \
+      if (fits) return launch_tma_pass<T, NN, AXIS, P>(g, kind, tb, ld.src, st, s, NoMul(), 0, 0, ks); \
       break;                                                                                           \
     }
     switch (n) {
@@ -559,6 +576,7 @@ cudaError_t launch_pass(const Geom& g, int kind, Tables<T> tb, LoadField<T> ld, 
     }
 #undef QUASI_TMA_CASE
   }
+  if (AXIS == 2 && ks) return launch_pass<T, AXIS, ShiftKLoad<T>, Store>(g, kind, tb, ShiftKLoad<T>{g, ld.src}, st, s);
   return launch_pass<T, AXIS, LoadField<T>, Store>(g, kind, tb, ld, st, s);
 }
 
@@ -574,7 +592,7 @@ struct MulLoad {
   __device__ T operator()(int i, int j, int k) const {
     const int i1 = i + di, j1 = j + dj;
     if (i1 >= g.nx || j1 >= g.ny) return T(0);
-    return T(double(src[lin(g, i1, j1, k)]) * mul(i, j, k));
+    return src[lin(g, i1, j1, k)] * mul(i, j, k);
   }
 };
 

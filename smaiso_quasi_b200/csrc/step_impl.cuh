@@ -13,6 +13,7 @@
 
 #include "r2r_pass.cuh"
 #include "yz_plane.cuh"
+#include "z_pass.cuh"
 
 namespace quasi {
 
@@ -23,6 +24,9 @@ struct StepCtx {
   Geom g;
   // per-axis wavenumbers, quasi.cpp:397-431 (DST index n carries mode n+1)
   const double *vqx, *vqy, *vqz, *vsx, *vsy, *vsz;
+  // the same tables in the storage type (the spectral multipliers of the
+  // x passes are evaluated in it)
+  const T *tqx, *tqy, *tqz, *tsx, *tsy, *tsz;
   double ep, alpha, beta, gamma, q0, kp, rho0, rho_s, rho_m, nu, dt, scale;
   int variant, divv_switch, n0;   // n0: planes per emulated MPI rank (quasi.cpp:1641-1690)
   const int* nloop;               // device step counter (the reference's nLoop)
@@ -55,57 +59,51 @@ __device__ __forceinline__ double mq2c(const StepCtx<T>& c, int i, int j, int k)
 }
 
 // ---------------------------------------------------------------------------
-// Spectral loaders (first, x-axis pass of inverse transforms)
+// Spectral multipliers of the OUTPUT index (i, j, k) for the x passes of the
+// inverse transforms, evaluated in the storage type from its own copy of the
+// wavenumber tables (read-only loads).
 // ---------------------------------------------------------------------------
-
-// ---------------------------------------------------------------------------
-// Spectral multipliers of the OUTPUT index (i, j, k) for the TMA x passes
-// (the loaders above, in the form the TMA pass applies them).
-// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T tq2(const StepCtx<T>& c, int i, int j, int k) {   // quasi.cpp:882
+  const T x = __ldg(c.tqx + i), y = __ldg(c.tqy + j), z = __ldg(c.tqz + k);
+  return x * x + y * y + z * z;
+}
 template <typename T> struct MDf {      // dfDlapPsi, quasi.cpp:1044
   static constexpr bool kActive = true;
   StepCtx<T> c;
-  __device__ double operator()(int i, int j, int k) const { return c.alpha * (c.q0 * c.q0 - mq2c(c, i, j, k)); }
+  __device__ T operator()(int i, int j, int k) const { return T(c.alpha) * (T(c.q0 * c.q0) - tq2(c, i, j, k)); }
 };
 template <typename T> struct MLap {     // lapRhoDfDlapPsi, quasi.cpp:1046-1047
   static constexpr bool kActive = true;
   StepCtx<T> c;
-  __device__ double operator()(int i, int j, int k) const {
-    const double q2 = mq2c(c, i, j, k);
-    return -q2 * (c.alpha * (c.q0 * c.q0 - q2));
+  __device__ T operator()(int i, int j, int k) const {
+    const T q2 = tq2(c, i, j, k);
+    return -q2 * (T(c.alpha) * (T(c.q0 * c.q0) - q2));
   }
 };
 template <typename T> struct MSh {      // -aLin, quasi-stb.cpp:1019
   static constexpr bool kActive = true;
   StepCtx<T> c;
-  __device__ double operator()(int i, int j, int k) const {
-    const double q2 = mq2c(c, i, j, k);
-    return -(c.ep - c.alpha * sq(c.q0 * c.q0 - q2));
+  __device__ T operator()(int i, int j, int k) const {
+    const T d = T(c.q0 * c.q0) - tq2(c, i, j, k);
+    return -(T(c.ep) - T(c.alpha) * (d * d));
   }
 };
 // Shifted gradient along A, quasi.cpp:1120-1186.  The input is read at
 // index + 1 along x or y by the TMA box offset (the row past the end reads as
-// zero: the reference's zero top DST index); along z the shift is applied
-// when storing (StShiftK), so the multiplier uses the output index k - 1.
+// zero: the reference's zero top DST index); along z the z pass shifts each
+// row by one when it stages it, so the multiplier here uses k - 1.
 template <typename T, int A, bool LAP> struct MGrad {
   static constexpr bool kActive = true;
   StepCtx<T> c;
-  __device__ double operator()(int i, int j, int k) const {
-    if (A == 2 && k == 0) return 0.0;
+  __device__ T operator()(int i, int j, int k) const {
+    if (A == 2 && k == 0) return T(0);
     const int ko = A == 2 ? k - 1 : k;
-    const double vs = A == 0 ? c.vsx[i] : (A == 1 ? c.vsy[j] : c.vsz[ko]);
+    const T vs = A == 0 ? __ldg(c.tsx + i) : (A == 1 ? __ldg(c.tsy + j) : __ldg(c.tsz + ko));
     if (!LAP) return -vs;
-    const double mq = (A == 0 ? sq(c.vsx[i]) : sq(c.vqx[i])) + (A == 1 ? sq(c.vsy[j]) : sq(c.vqy[j])) +
-                      (A == 2 ? sq(c.vsz[ko]) : sq(c.vqz[ko]));
-    return mq * vs;   // -mq * (-vs)
-  }
-};
-template <typename T> struct StShiftK {   // value of input k lands at k - 1; k = 0 zeroes nz - 1
-  Geom g;
-  T* dst;
-  __device__ void operator()(int i, int j, int k, T v) const {
-    if (k == 0) dst[lin(g, i, j, g.nz - 1)] = T(0);
-    else dst[lin(g, i, j, k - 1)] = v;
+    const T a = A == 0 ? vs : __ldg(c.tqx + i), b = A == 1 ? vs : __ldg(c.tqy + j),
+            d = A == 2 ? vs : __ldg(c.tqz + ko);
+    return (a * a + b * b + d * d) * vs;   // -mq * (-vs)
   }
 };
 
@@ -126,9 +124,16 @@ template <typename T> struct LdRealField {
 // rhoq = scale CT(rho) exp(-1.57^2 q^2 8)                     quasi.cpp:1260-1261
 template <typename T> struct StRhoq {
   StepCtx<T> c;
-  __device__ void operator()(int i, int j, int k, T v) const {
-    const double q2 = mq2c(c, i, j, k);
-    c.rhoq[at(c, i, j, k)] = T(c.scale * double(v) * exp(-1.57 * 1.57 * q2 * 8));
+  __device__ T value(int i, int j, int k, T v) const {
+    using A = Arith<T>;
+    return T(A(c.scale) * A(v) * exp(A(-1.57 * 1.57) * tq2(c, i, j, k) * A(8)));
+  }
+  __device__ void operator()(int i, int j, int k, T v) const { c.rhoq[at(c, i, j, k)] = value(i, j, k, v); }
+  __device__ void pair(int i, int j, int k, T a, T b) const {
+    typename Vec2<T>::type v;
+    v.x = value(i, j, k, a);
+    v.y = value(i, j, k + 1, b);
+    *reinterpret_cast<typename Vec2<T>::type*>(c.rhoq + at(c, i, j, k)) = v;
   }
 };
 
@@ -490,16 +495,25 @@ struct AxisTables {
 
 // y and z passes of `src` (plain field) into `st`: one cluster pass when the
 // plane shape allows it, else two passes (the second in place on st.dst).
+// kshift = 1: the z pass transforms row[k + 1] (zero at the top) in place of
+// row[k], the z shift of a z gradient (quasi.cpp:1163-1186).
 template <typename T, class Store>
-cudaError_t yz3(const Geom& g, const AxisTables<T>& tb, const int kinds[3], T* src, Store st, cudaStream_t s) {
+cudaError_t yz3(const Geom& g, const AxisTables<T>& tb, const int kinds[3], T* src, Store st, cudaStream_t s,
+                int kshift = 0) {
   if constexpr (IsStoreField<Store>::value) {
-    cudaError_t e = launch_yz<T>(g, kinds[1], kinds[2], tb.t[1], tb.t[2], src, st.dst, s);
-    if (e != cudaErrorNotSupported) return e;
+    if (!kshift) {
+      cudaError_t e = launch_yz<T>(g, kinds[1], kinds[2], tb.t[1], tb.t[2], src, st.dst, s);
+      if (e != cudaErrorNotSupported) return e;
+    }
   }
   cudaError_t e;
   if ((e = launch_pass<T, 1>(g, kinds[1], tb.t[1], LoadField<T>{g, src}, StoreField<T>{g, src}, s)) != cudaSuccess)
     return e;
-  return launch_pass<T, 2>(g, kinds[2], tb.t[2], LoadField<T>{g, src}, st, s);
+  if constexpr (IsStoreField<Store>::value) {
+    e = launch_zpass<T>(g, kinds[2], tb.t[2], src, st.dst, s, kshift);
+    if (e != cudaErrorNotSupported) return e;
+  }
+  return launch_pass<T, 2>(g, kinds[2], tb.t[2], LoadField<T>{g, src}, st, s, kshift);
 }
 
 // Inverse: x pass (loader -> dst), then y and z (storer).
@@ -511,14 +525,15 @@ cudaError_t inverse3(const Geom& g, const AxisTables<T>& tb, const int kinds[3],
   return yz3(g, tb, kinds, dst, st, s);
 }
 
-// Inverse with a spectral multiplier: x pass on mul * src[shifted] -> dst
-// through stx, then plain y and z passes in place.
+// Inverse with a spectral multiplier: x pass on mul * src[i + di, j + dj,
+// k + dk] -> dst through stx, then plain y and z passes in place (the z pass
+// applies dk).
 template <typename T, class Mul, class StX>
 cudaError_t inverse3_mul(const Geom& g, const AxisTables<T>& tb, const int kinds[3], const T* src, Mul mul, int di,
-                         int dj, StX stx, T* dst, cudaStream_t s) {
+                         int dj, int dk, StX stx, T* dst, cudaStream_t s) {
   cudaError_t e;
   if ((e = launch_mul_x_pass<T>(g, kinds[0], tb.t[0], src, mul, di, dj, stx, s)) != cudaSuccess) return e;
-  return yz3(g, tb, kinds, dst, StoreField<T>{g, dst}, s);
+  return yz3(g, tb, kinds, dst, StoreField<T>{g, dst}, s, dk);
 }
 
 // Forward: z and y (loader -> dst), then x pass (storer).  A plain field
@@ -536,7 +551,10 @@ cudaError_t forward3(const Geom& g, const AxisTables<T>& tb, const int kinds[3],
     }
   }
   if (!fused) {
-    if ((e = launch_pass<T, 2>(g, kinds[2], tb.t[2], ld, StoreField<T>{g, dst}, s)) != cudaSuccess) return e;
+    e = cudaErrorNotSupported;
+    if constexpr (std::is_same<Load, LoadField<T>>::value) e = launch_zpass<T>(g, kinds[2], tb.t[2], ld.src, dst, s);
+    if (e == cudaErrorNotSupported) e = launch_pass<T, 2>(g, kinds[2], tb.t[2], ld, StoreField<T>{g, dst}, s);
+    if (e != cudaSuccess) return e;
     if ((e = launch_pass<T, 1>(g, kinds[1], tb.t[1], LoadField<T>{g, dst}, StoreField<T>{g, dst}, s)) != cudaSuccess)
       return e;
   }
@@ -593,18 +611,18 @@ cudaError_t enqueue_step(const StepCtx<T>& c, const AxisTables<T>& tb, int* nloo
   auto ld = [&](T* d) { return LoadField<T>{g, d}; };
   if (c.variant == kQuasi) {
     // a3 prologue quasi.cpp:1036-1057
-    QUASI_TRY(inverse3_mul(g, tb, kiCT, c.psiq, MDf<T>{c}, 0, 0, st(c.df), c.df, s));
-    QUASI_TRY(inverse3_mul(g, tb, kiCT, c.psiq, MLap<T>{c}, 0, 0, st(c.lap), c.lap, s));
+    QUASI_TRY(inverse3_mul(g, tb, kiCT, c.psiq, MDf<T>{c}, 0, 0, 0, st(c.df), c.df, s));
+    QUASI_TRY(inverse3_mul(g, tb, kiCT, c.psiq, MLap<T>{c}, 0, 0, 0, st(c.lap), c.lap, s));
     // a4 gradients quasi.cpp:1120-1232
-    QUASI_TRY(inverse3_mul(g, tb, kiSTx, c.psiq, MGrad<T, 0, false>{c}, 1, 0, st(c.gx), c.gx, s));
-    QUASI_TRY(inverse3_mul(g, tb, kiSTy, c.psiq, MGrad<T, 1, false>{c}, 0, 1, st(c.gy), c.gy, s));
-    QUASI_TRY(inverse3_mul(g, tb, kiSTz, c.psiq, MGrad<T, 2, false>{c}, 0, 0, StShiftK<T>{g, c.gz}, c.gz, s));
-    QUASI_TRY(inverse3_mul(g, tb, kiSTx, c.rhoq, MGrad<T, 0, false>{c}, 1, 0, st(c.rdx), c.rdx, s));
-    QUASI_TRY(inverse3_mul(g, tb, kiSTy, c.rhoq, MGrad<T, 1, false>{c}, 0, 1, st(c.rdy), c.rdy, s));
-    QUASI_TRY(inverse3_mul(g, tb, kiSTz, c.rhoq, MGrad<T, 2, false>{c}, 0, 0, StShiftK<T>{g, c.rdz}, c.rdz, s));
-    QUASI_TRY(inverse3_mul(g, tb, kiSTx, c.psiq, MGrad<T, 0, true>{c}, 1, 0, st(c.ldx), c.ldx, s));
-    QUASI_TRY(inverse3_mul(g, tb, kiSTy, c.psiq, MGrad<T, 1, true>{c}, 0, 1, st(c.ldy), c.ldy, s));
-    QUASI_TRY(inverse3_mul(g, tb, kiSTz, c.psiq, MGrad<T, 2, true>{c}, 0, 0, StShiftK<T>{g, c.ldz}, c.ldz, s));
+    QUASI_TRY(inverse3_mul(g, tb, kiSTx, c.psiq, MGrad<T, 0, false>{c}, 1, 0, 0, st(c.gx), c.gx, s));
+    QUASI_TRY(inverse3_mul(g, tb, kiSTy, c.psiq, MGrad<T, 1, false>{c}, 0, 1, 0, st(c.gy), c.gy, s));
+    QUASI_TRY(inverse3_mul(g, tb, kiSTz, c.psiq, MGrad<T, 2, false>{c}, 0, 0, 1, st(c.gz), c.gz, s));
+    QUASI_TRY(inverse3_mul(g, tb, kiSTx, c.rhoq, MGrad<T, 0, false>{c}, 1, 0, 0, st(c.rdx), c.rdx, s));
+    QUASI_TRY(inverse3_mul(g, tb, kiSTy, c.rhoq, MGrad<T, 1, false>{c}, 0, 1, 0, st(c.rdy), c.rdy, s));
+    QUASI_TRY(inverse3_mul(g, tb, kiSTz, c.rhoq, MGrad<T, 2, false>{c}, 0, 0, 1, st(c.rdz), c.rdz, s));
+    QUASI_TRY(inverse3_mul(g, tb, kiSTx, c.psiq, MGrad<T, 0, true>{c}, 1, 0, 0, st(c.ldx), c.ldx, s));
+    QUASI_TRY(inverse3_mul(g, tb, kiSTy, c.psiq, MGrad<T, 1, true>{c}, 0, 1, 0, st(c.ldy), c.ldy, s));
+    QUASI_TRY(inverse3_mul(g, tb, kiSTz, c.psiq, MGrad<T, 2, true>{c}, 0, 0, 1, st(c.ldz), c.ldz, s));
     // a5 density + filter quasi.cpp:1237-1268 (rho doubles as the scratch)
     QUASI_EW(rho_law_kernel<T>, c, n);
     QUASI_TRY(cudaGetLastError());
@@ -616,10 +634,10 @@ cudaError_t enqueue_step(const StepCtx<T>& c, const AxisTables<T>& tb, int* nloo
     QUASI_TRY(forward3(g, tb, kCT, ld(c.divv), c.divvq, st(c.divvq), s));
   } else {
     // quasi-stb.cpp:1005-1038 (the unused dRho transform is elided)
-    QUASI_TRY(inverse3_mul(g, tb, kiCT, c.psiq, MSh<T>{c}, 0, 0, st(c.sh), c.sh, s));
-    QUASI_TRY(inverse3_mul(g, tb, kiSTx, c.psiq, MGrad<T, 0, false>{c}, 1, 0, st(c.gx), c.gx, s));
-    QUASI_TRY(inverse3_mul(g, tb, kiSTy, c.psiq, MGrad<T, 1, false>{c}, 0, 1, st(c.gy), c.gy, s));
-    QUASI_TRY(inverse3_mul(g, tb, kiSTz, c.psiq, MGrad<T, 2, false>{c}, 0, 0, StShiftK<T>{g, c.gz}, c.gz, s));
+    QUASI_TRY(inverse3_mul(g, tb, kiCT, c.psiq, MSh<T>{c}, 0, 0, 0, st(c.sh), c.sh, s));
+    QUASI_TRY(inverse3_mul(g, tb, kiSTx, c.psiq, MGrad<T, 0, false>{c}, 1, 0, 0, st(c.gx), c.gx, s));
+    QUASI_TRY(inverse3_mul(g, tb, kiSTy, c.psiq, MGrad<T, 1, false>{c}, 0, 1, 0, st(c.gy), c.gy, s));
+    QUASI_TRY(inverse3_mul(g, tb, kiSTz, c.psiq, MGrad<T, 2, false>{c}, 0, 0, 1, st(c.gz), c.gz, s));
     // rho == 1, divv == 0, grad rho == 0 (rhoq never leaves 0): quasi-stb.cpp:1232
   }
   // a7 stress quasi.cpp:1298-1330
