@@ -132,15 +132,16 @@ def make_sim(q, prec: str, device: int):
 
 
 def run_profile_case(args) -> None:
-    """The FP32 engine alone (about 2.3 GB on the device): W + K steps and the
-    timed plain y pass, the case the committed ncu summaries capture."""
+    """One engine alone (FP32: about 2.3 GB on the device, FP64 about 4.6 GB):
+    W + K steps, then 1 + 3 launches of the plain pass along --axis, the case
+    the committed ncu summaries capture."""
     import smaiso_quasi_b200 as q
-    cfg, sim = make_sim(q, "fp32", 0)
+    cfg, sim = make_sim(q, args.precision, 0)
     sim.set_psi(q.initial_condition(cfg, "planar", seed=1234))
     sim.init()
     sim.step(args.warmup + args.steps)
-    print(json.dumps({"profile_case": "fp32 256^3", "steps": args.warmup + args.steps,
-                      "y_pass_ms": sim.time_axis_pass(1, reps=3)}))
+    print(json.dumps({"profile_case": f"{args.precision} 256^3", "steps": args.warmup + args.steps,
+                      "axis": args.axis, "pass_ms": sim.time_axis_pass(args.axis, reps=3)}))
 
 
 def run_gpu(args) -> None:
@@ -316,7 +317,9 @@ def main():
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--err-steps", type=int, default=1000, help="steps after which FP32 is compared with FP64")
-    ap.add_argument("--profile", action="store_true", help="FP32 engine only (for ncu captures)")
+    ap.add_argument("--profile", action="store_true", help="one engine only (for ncu captures)")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"], help="engine of --profile")
+    ap.add_argument("--axis", type=int, default=1, choices=[0, 1, 2], help="pass timed at the end of --profile")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -198,6 +198,26 @@ typedef struct quasi_ic {
 QUASI_API int quasi_ic_default(quasi_ic* ic, int kind);
 QUASI_API int quasi_initial_condition(const quasi_config* cfg, const quasi_ic* ic, double* host_psi);
 
+/* ---- ensembles of independent instances ------------------------------------
+ * n members, each an instance with its own grid, variant, precision, device
+ * and constants (configs[m]), stepped together: quasi_ensemble_step enqueues
+ * nsteps on every member's stream before it waits for any, so the members
+ * share the GPU(s).  Members are reached through quasi_ensemble_member (a
+ * handle owned by the ensemble: set_psi, get_field, diagnostics, growth rate,
+ * save/load; do not destroy it).  No reference counterpart: the reference
+ * runs one instance per MPI job (quasi-stb.cpp:2113-2159 is its growth-rate
+ * probe). */
+typedef struct quasi_ensemble quasi_ensemble;
+QUASI_API int quasi_ensemble_create(int n, const quasi_config* configs, quasi_ensemble** out);
+QUASI_API int quasi_ensemble_size(const quasi_ensemble* e, int* n);
+QUASI_API int quasi_ensemble_member(quasi_ensemble* e, int m, quasi_handle** out);
+/* quasi_init of every member (each must have had quasi_set_psi). */
+QUASI_API int quasi_ensemble_init(quasi_ensemble* e);
+QUASI_API int quasi_ensemble_step(quasi_ensemble* e, int nsteps);
+/* quasi_growth_rate of every member into out[0..n-1] (quasi-stb members). */
+QUASI_API int quasi_ensemble_growth_rates(quasi_ensemble* e, double* out);
+QUASI_API int quasi_ensemble_destroy(quasi_ensemble* e);
+
 /* ---- lower interface: one 3-D r2r transform with FFTW semantics ---------
  * kind[a] per axis (x, y, z): 0 REDFT10, 1 REDFT01, 2 RODFT10, 3 RODFT01,
  * unnormalised, in place.  Replaces fftw_mpi_plan_r2r_3d / fftw_execute

@@ -3,6 +3,7 @@
 
 #include <new>
 #include <string>
+#include <vector>
 
 #include "engine.cuh"
 
@@ -186,6 +187,109 @@ int quasi_save(quasi_handle* h, const char* path) {
 int quasi_load(quasi_handle* h, const char* path) {
   if (!path) return fail(QUASI_ERR_INVALID, "null path");
   QUASI_CALL(h, h->eng->load(path));
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Ensembles: a vector of owned handles stepped together.
+// ---------------------------------------------------------------------------
+struct quasi_ensemble {
+  std::vector<quasi_handle*> members;
+};
+
+namespace {
+
+int member_fail(size_t m, int rc) {
+  return fail(rc, "ensemble member " + std::to_string(m) + ": " + g_err);
+}
+
+}  // namespace
+
+extern "C" {
+
+int quasi_ensemble_create(int n, const quasi_config* configs, quasi_ensemble** out) {
+  if (!out || !configs || n < 1) return fail(QUASI_ERR_INVALID, "need n >= 1 configs and an output pointer");
+  *out = nullptr;
+  auto* e = new (std::nothrow) quasi_ensemble;
+  if (!e) return fail(QUASI_ERR_NOMEM, "host allocation failed");
+  for (int m = 0; m < n; ++m) {
+    quasi_handle* h = nullptr;
+    int rc = quasi_create(&configs[m], &h);
+    if (rc) {
+      rc = member_fail(m, rc);
+      quasi_ensemble_destroy(e);
+      return rc;
+    }
+    e->members.push_back(h);
+  }
+  *out = e;
+  return QUASI_OK;
+}
+
+int quasi_ensemble_size(const quasi_ensemble* e, int* n) {
+  if (!e || !n) return fail(QUASI_ERR_INVALID, "null argument");
+  *n = int(e->members.size());
+  return QUASI_OK;
+}
+
+int quasi_ensemble_member(quasi_ensemble* e, int m, quasi_handle** out) {
+  if (!e || !out) return fail(QUASI_ERR_INVALID, "null argument");
+  if (m < 0 || m >= int(e->members.size())) return fail(QUASI_ERR_INVALID, "member index out of range");
+  *out = e->members[m];
+  return QUASI_OK;
+}
+
+int quasi_ensemble_init(quasi_ensemble* e) {
+  if (!e) return fail(QUASI_ERR_INVALID, "null ensemble");
+  for (size_t m = 0; m < e->members.size(); ++m) {
+    int rc = quasi_init(e->members[m]);
+    if (rc) return member_fail(m, rc);
+  }
+  return QUASI_OK;
+}
+
+int quasi_ensemble_step(quasi_ensemble* e, int nsteps) {
+  if (!e) return fail(QUASI_ERR_INVALID, "null ensemble");
+  if (nsteps < 0) return fail(QUASI_ERR_INVALID, "nsteps < 0");
+  // enqueue everything first; then wait for every member (all of them, even
+  // after an error, so that no member is left running)
+  int first = QUASI_OK;
+  std::string first_err;
+  size_t enq = 0;
+  for (; enq < e->members.size(); ++enq) {
+    int rc = quasi_step_async(e->members[enq], nsteps);
+    if (rc) {
+      first = member_fail(enq, rc);
+      first_err = g_err;
+      break;
+    }
+  }
+  for (size_t m = 0; m < enq; ++m) {
+    int rc = quasi_synchronize(e->members[m]);
+    if (rc && first == QUASI_OK) {
+      first = member_fail(m, rc);
+      first_err = g_err;
+    }
+  }
+  if (first) g_err = first_err;
+  return first;
+}
+
+int quasi_ensemble_growth_rates(quasi_ensemble* e, double* out) {
+  if (!e || !out) return fail(QUASI_ERR_INVALID, "null argument");
+  for (size_t m = 0; m < e->members.size(); ++m) {
+    int rc = quasi_growth_rate(e->members[m], &out[m]);
+    if (rc) return member_fail(m, rc);
+  }
+  return QUASI_OK;
+}
+
+int quasi_ensemble_destroy(quasi_ensemble* e) {
+  if (!e) return QUASI_OK;
+  for (quasi_handle* h : e->members) quasi_destroy(h);
+  delete e;
+  return QUASI_OK;
 }
 
 }  // extern "C"

@@ -115,11 +115,11 @@ class Engine : public EngineBase {
       for (int i = 0; i < n; ++i) h.push_back(1.0 * M_PI * i / (d * n));
       for (int i = 0; i < n; ++i) h.push_back(1.0 * M_PI * (i + 1) / (d * n));
     }
-    // doubles, then the same values in the storage type
-    std::vector<T> ht(h.begin(), h.end());
-    if (!cuda_ok(cudaMalloc(&tabs_, h.size() * (sizeof(double) + sizeof(T))), "malloc")) return QUASI_ERR_CUDA;
-    if (!cuda_ok(cudaMemcpy(tabs_, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice), "memcpy") ||
-        !cuda_ok(cudaMemcpy(tabs_ + h.size(), ht.data(), ht.size() * sizeof(T), cudaMemcpyHostToDevice), "memcpy"))
+    // then the density filter per axis, exp(-1.57^2 8 vq^2) (quasi.cpp:1260)
+    for (int a = 0, off = 0; a < 3; off += 2 * len[a], ++a)
+      for (int i = 0; i < len[a]; ++i) h.push_back(std::exp(-1.57 * 1.57 * 8 * h[off + i] * h[off + i]));
+    if (!cuda_ok(cudaMalloc(&tabs_, h.size() * sizeof(double)), "malloc")) return QUASI_ERR_CUDA;
+    if (!cuda_ok(cudaMemcpy(tabs_, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice), "memcpy"))
       return QUASI_ERR_CUDA;
     for (int a = 0; a < 3; ++a)
       if (!cuda_ok(tw_[a].upload(len[a]), "twiddles")) return QUASI_ERR_CUDA;
@@ -367,10 +367,11 @@ class Engine : public EngineBase {
     c_.vqx = t;                 c_.vsx = t + g_.nx;
     c_.vqy = t + 2 * g_.nx;     c_.vsy = c_.vqy + g_.ny;
     c_.vqz = t + 2 * g_.nx + 2 * g_.ny; c_.vsz = c_.vqz + g_.nz;
-    const T* tt = reinterpret_cast<const T*>(tabs_ + h.size());
-    c_.tqx = tt;                 c_.tsx = tt + g_.nx;
-    c_.tqy = tt + 2 * g_.nx;     c_.tsy = c_.tqy + g_.ny;
-    c_.tqz = tt + 2 * g_.nx + 2 * g_.ny; c_.tsz = c_.tqz + g_.nz;
+    const double* ft = t + 2 * (g_.nx + g_.ny + g_.nz);
+    c_.fx = ft;
+    c_.fy = ft + g_.nx;
+    c_.fz = ft + g_.nx + g_.ny;
+    (void)h;
     const bool quasi = cfg_.variant == QUASI_VARIANT_QUASI;
     c_.ep = -0.001 * cfg_.ep_arg;                                   // quasi.cpp:187
     c_.alpha = cfg_.alpha; c_.beta = cfg_.beta; c_.gamma = cfg_.gamma; c_.q0 = cfg_.q0;

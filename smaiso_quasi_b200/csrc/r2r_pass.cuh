@@ -275,8 +275,9 @@ struct MulSrc {
     if constexpr (Mul::kActive) {
       const int k = k0 + 2 * g;
       const int i = AXIS == 1 ? outer : n, j = AXIS == 1 ? n : outer;
-      a = a * mul(i, j, k);
-      b = b * mul(i, j, k + 1);
+      using M = decltype(mul(i, j, k));   // the multiplier's own type
+      a = T(M(a) * mul(i, j, k));
+      b = T(M(b) * mul(i, j, k + 1));
     }
   }
 };
@@ -592,7 +593,8 @@ struct MulLoad {
   __device__ T operator()(int i, int j, int k) const {
     const int i1 = i + di, j1 = j + dj;
     if (i1 >= g.nx || j1 >= g.ny) return T(0);
-    return src[lin(g, i1, j1, k)] * mul(i, j, k);
+    using M = decltype(mul(i, j, k));
+    return T(M(src[lin(g, i1, j1, k)]) * mul(i, j, k));
   }
 };
 

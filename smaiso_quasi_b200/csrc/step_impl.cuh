@@ -24,9 +24,8 @@ struct StepCtx {
   Geom g;
   // per-axis wavenumbers, quasi.cpp:397-431 (DST index n carries mode n+1)
   const double *vqx, *vqy, *vqz, *vsx, *vsy, *vsz;
-  // the same tables in the storage type (the spectral multipliers of the
-  // x passes are evaluated in it)
-  const T *tqx, *tqy, *tqz, *tsx, *tsy, *tsz;
+  // the density filter exp(-1.57^2 8 q^2) per axis: exp(-1.57^2 8 vq_a^2)
+  const double *fx, *fy, *fz;
   double ep, alpha, beta, gamma, q0, kp, rho0, rho_s, rho_m, nu, dt, scale;
   int variant, divv_switch, n0;   // n0: planes per emulated MPI rank (quasi.cpp:1641-1690)
   const int* nloop;               // device step counter (the reference's nLoop)
@@ -60,33 +59,33 @@ __device__ __forceinline__ double mq2c(const StepCtx<T>& c, int i, int j, int k)
 
 // ---------------------------------------------------------------------------
 // Spectral multipliers of the OUTPUT index (i, j, k) for the x passes of the
-// inverse transforms, evaluated in the storage type from its own copy of the
-// wavenumber tables (read-only loads).
+// inverse transforms, in double (the x pass rounds the product once).  The
+// spectrum concentrates on the ring |q| = q0, where q0^2 - q^2 cancels.
 // ---------------------------------------------------------------------------
 template <typename T>
-__device__ __forceinline__ T tq2(const StepCtx<T>& c, int i, int j, int k) {   // quasi.cpp:882
-  const T x = __ldg(c.tqx + i), y = __ldg(c.tqy + j), z = __ldg(c.tqz + k);
+__device__ __forceinline__ double dq2(const StepCtx<T>& c, int i, int j, int k) {   // quasi.cpp:882
+  const double x = __ldg(c.vqx + i), y = __ldg(c.vqy + j), z = __ldg(c.vqz + k);
   return x * x + y * y + z * z;
 }
 template <typename T> struct MDf {      // dfDlapPsi, quasi.cpp:1044
   static constexpr bool kActive = true;
   StepCtx<T> c;
-  __device__ T operator()(int i, int j, int k) const { return T(c.alpha) * (T(c.q0 * c.q0) - tq2(c, i, j, k)); }
+  __device__ double operator()(int i, int j, int k) const { return c.alpha * (c.q0 * c.q0 - dq2(c, i, j, k)); }
 };
 template <typename T> struct MLap {     // lapRhoDfDlapPsi, quasi.cpp:1046-1047
   static constexpr bool kActive = true;
   StepCtx<T> c;
-  __device__ T operator()(int i, int j, int k) const {
-    const T q2 = tq2(c, i, j, k);
-    return -q2 * (T(c.alpha) * (T(c.q0 * c.q0) - q2));
+  __device__ double operator()(int i, int j, int k) const {
+    const double q2 = dq2(c, i, j, k);
+    return -q2 * (c.alpha * (c.q0 * c.q0 - q2));
   }
 };
 template <typename T> struct MSh {      // -aLin, quasi-stb.cpp:1019
   static constexpr bool kActive = true;
   StepCtx<T> c;
-  __device__ T operator()(int i, int j, int k) const {
-    const T d = T(c.q0 * c.q0) - tq2(c, i, j, k);
-    return -(T(c.ep) - T(c.alpha) * (d * d));
+  __device__ double operator()(int i, int j, int k) const {
+    const double d = c.q0 * c.q0 - dq2(c, i, j, k);
+    return -(c.ep - c.alpha * (d * d));
   }
 };
 // Shifted gradient along A, quasi.cpp:1120-1186.  The input is read at
@@ -96,13 +95,13 @@ template <typename T> struct MSh {      // -aLin, quasi-stb.cpp:1019
 template <typename T, int A, bool LAP> struct MGrad {
   static constexpr bool kActive = true;
   StepCtx<T> c;
-  __device__ T operator()(int i, int j, int k) const {
-    if (A == 2 && k == 0) return T(0);
+  __device__ double operator()(int i, int j, int k) const {
+    if (A == 2 && k == 0) return 0.0;
     const int ko = A == 2 ? k - 1 : k;
-    const T vs = A == 0 ? __ldg(c.tsx + i) : (A == 1 ? __ldg(c.tsy + j) : __ldg(c.tsz + ko));
+    const double vs = A == 0 ? __ldg(c.vsx + i) : (A == 1 ? __ldg(c.vsy + j) : __ldg(c.vsz + ko));
     if (!LAP) return -vs;
-    const T a = A == 0 ? vs : __ldg(c.tqx + i), b = A == 1 ? vs : __ldg(c.tqy + j),
-            d = A == 2 ? vs : __ldg(c.tqz + ko);
+    const double a = A == 0 ? vs : __ldg(c.vqx + i), b = A == 1 ? vs : __ldg(c.vqy + j),
+                 d = A == 2 ? vs : __ldg(c.vqz + ko);
     return (a * a + b * b + d * d) * vs;   // -mq * (-vs)
   }
 };
@@ -122,11 +121,13 @@ template <typename T> struct LdRealField {
 // ---------------------------------------------------------------------------
 
 // rhoq = scale CT(rho) exp(-1.57^2 q^2 8)                     quasi.cpp:1260-1261
+// (the Gaussian as the product of its per-axis factors, in double, with one
+// rounding to the storage type: rho's rounding noise is what the divv
+// difference quotient (rho - rho_old) / dt amplifies)
 template <typename T> struct StRhoq {
   StepCtx<T> c;
   __device__ T value(int i, int j, int k, T v) const {
-    using A = Arith<T>;
-    return T(A(c.scale) * A(v) * exp(A(-1.57 * 1.57) * tq2(c, i, j, k) * A(8)));
+    return T(c.scale * double(v) * (__ldg(c.fx + i) * __ldg(c.fy + j) * __ldg(c.fz + k)));
   }
   __device__ void operator()(int i, int j, int k, T v) const { c.rhoq[at(c, i, j, k)] = value(i, j, k, v); }
   __device__ void pair(int i, int j, int k, T a, T b) const {

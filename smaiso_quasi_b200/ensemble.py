@@ -72,27 +72,22 @@ def run_members(members: list[Member], steps: int, precision: str = "fp32", devi
     """Advance every member `steps` steps concurrently; returns growth rates
     (the quasi-stb probe at the perturbation's mode) and device-side timing."""
     from . import quasi as q
-    sims = []
-    for mb in members:
-        cfg = q.default_config("stb", *mb.grid, precision=precision, device=device, q_pert=mb.q_h())
-        s = q.Simulation(cfg)
+    cfgs = [q.default_config("stb", *mb.grid, precision=precision, device=device, q_pert=mb.q_h())
+            for mb in members]
+    ens = q.Ensemble(cfgs)   # quasi_ensemble_create
+    for mb, cfg, s in zip(members, cfgs, ens.members):
         s.set_psi(q.initial_condition(cfg, "interface", seed=mb.seed, eps_h=mb.eps_h, q_h=mb.q_h()))
-        s.init()
-        sims.append(s)
+    ens.init()
     t0 = time.perf_counter()
     done = 0
     while done < steps:
         n = min(chunk, steps - done)
-        for s in sims:
-            s.step_async(n)
-        for s in sims:
-            s.synchronize()
+        ens.step(n)   # every member enqueued before any is waited for
         done += n
     wall = time.perf_counter() - t0
-    growth = [s.growth_rate() for s in sims]
+    growth = [float(v) for v in ens.growth_rates()]
     cells = sum(mb.cells for mb in members)
-    for s in sims:
-        s.close()
+    ens.close()
     return {"indices": [mb.index for mb in members], "growth": growth, "wall_s": wall,
             "instance_steps_per_s": len(members) * steps / wall if wall > 0 else 0.0,
             "cell_updates_per_s": cells * steps / wall if wall > 0 else 0.0}

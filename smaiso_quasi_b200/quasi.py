@@ -37,6 +37,8 @@ EXPORTS = [
     "quasi_r2r_execute_device", "quasi_r2r_execute_host", "quasi_r2r_plan_destroy",
     "quasi_ic_default", "quasi_initial_condition", "quasi_step_kernels", "quasi_time_axis_pass",
     "quasi_step_async", "quasi_synchronize", "quasi_diagnostics_noalloc",
+    "quasi_ensemble_create", "quasi_ensemble_size", "quasi_ensemble_member", "quasi_ensemble_init",
+    "quasi_ensemble_step", "quasi_ensemble_growth_rates", "quasi_ensemble_destroy",
 ]
 IC_KIND = {"planar": 0, "undulated": 1, "interface": 2, "droplet": 3, "stb": 4, "focal_conic": 5}
 
@@ -107,6 +109,13 @@ def lib() -> ctypes.CDLL:
         L.quasi_time_axis_pass.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, dp]
         L.quasi_ic_default.argtypes = [ctypes.POINTER(IC), ctypes.c_int]
         L.quasi_initial_condition.argtypes = [ctypes.POINTER(Config), ctypes.POINTER(IC), dp]
+        L.quasi_ensemble_create.argtypes = [ctypes.c_int, ctypes.POINTER(Config), ctypes.POINTER(ctypes.c_void_p)]
+        L.quasi_ensemble_size.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
+        L.quasi_ensemble_member.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+        L.quasi_ensemble_init.argtypes = [ctypes.c_void_p]
+        L.quasi_ensemble_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.quasi_ensemble_growth_rates.argtypes = [ctypes.c_void_p, dp]
+        L.quasi_ensemble_destroy.argtypes = [ctypes.c_void_p]
         _lib = L
     return _lib
 
@@ -144,16 +153,21 @@ def initial_condition(cfg: Config, kind: str = "planar", **params) -> np.ndarray
 class Simulation:
     """One instance of the step on one GPU (a ``quasi_handle``)."""
 
-    def __init__(self, cfg: Config):
+    def __init__(self, cfg: Config, _handle=None, _owner=None):
         self.cfg = cfg
         self.shape = (cfg.nx, cfg.ny, cfg.nz)
+        self._owner = _owner   # an Ensemble that owns the handle, else None
+        if _handle is not None:
+            self._h = _handle
+            return
         h = ctypes.c_void_p()
         _check(lib().quasi_create(ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h
 
     def close(self) -> None:
         if getattr(self, "_h", None):
-            lib().quasi_destroy(self._h)
+            if self._owner is None:
+                lib().quasi_destroy(self._h)
             self._h = None
 
     def __enter__(self):
@@ -228,6 +242,58 @@ class Simulation:
 
     def load(self, path: str) -> None:
         _check(lib().quasi_load(self._h, str(path).encode()))
+
+
+class Ensemble:
+    """Independent instances stepped together (a ``quasi_ensemble``): every
+    member's steps are enqueued on its own stream before any is waited for.
+    ``members[m]`` is a Simulation view of member m (owned by the ensemble)."""
+
+    def __init__(self, configs: list[Config]):
+        arr = (Config * len(configs))(*configs)
+        h = ctypes.c_void_p()
+        _check(lib().quasi_ensemble_create(len(configs), arr, ctypes.byref(h)))
+        self._h = h
+        self.members = []
+        for m, cfg in enumerate(configs):
+            mh = ctypes.c_void_p()
+            _check(lib().quasi_ensemble_member(self._h, m, ctypes.byref(mh)))
+            self.members.append(Simulation(cfg, _handle=mh, _owner=self))
+
+    def __len__(self) -> int:
+        n = ctypes.c_int()
+        _check(lib().quasi_ensemble_size(self._h, ctypes.byref(n)))
+        return n.value
+
+    def init(self) -> None:
+        _check(lib().quasi_ensemble_init(self._h))
+
+    def step(self, n: int = 1) -> None:
+        _check(lib().quasi_ensemble_step(self._h, int(n)))
+
+    def growth_rates(self) -> np.ndarray:
+        out = np.zeros(len(self.members))
+        _check(lib().quasi_ensemble_growth_rates(self._h, _dptr(out)))
+        return out
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            for s in self.members:
+                s._h = None
+            lib().quasi_ensemble_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class R2RPlan:

@@ -91,3 +91,18 @@ def test_noise_stream_matches_the_oracle_exactly():
     a = q.initial_condition(cfg, "planar", seed=99, noise=1e-3, amp0=1e-300)
     b = (2.0 * qo.splitmix_uniform(99, 16 ** 3) - 1.0).reshape(16, 16, 16) * 1e-3
     np.testing.assert_allclose(a, b, rtol=0, atol=1e-18)
+
+
+def test_ensemble_rejects_a_bad_member_and_names_it():
+    """quasi_ensemble_create validates every member before touching a device;
+    the error names the failing member."""
+    import smaiso_quasi_b200 as q
+    good = q.default_config("stb", 16, 16, 32)
+    bad = q.default_config("stb", 16, 16, 33)
+    with pytest.raises(q.QuasiError) as ei:
+        q.Ensemble([bad, good])
+    assert "ensemble member 0" in str(ei.value)
+    lib = q.lib()
+    h = ctypes.c_void_p()
+    assert lib.quasi_ensemble_create(0, None, ctypes.byref(h)) != 0
+    assert lib.quasi_ensemble_destroy(None) == 0
