@@ -284,10 +284,12 @@ struct MulSrc {
 
 constexpr uint32_t kTmaPollLimit = 1u << 24;
 
+// Axes (bit 0: x, bit 1: y) whose TMA passes transform in place in the
+// landing buffer (see tma_pass_kernel's IP).
 #ifndef QUASI_TMA_INPLACE
 #define QUASI_TMA_INPLACE 0
 #endif
-constexpr bool kTmaInPlace = QUASI_TMA_INPLACE != 0;
+template <int AXIS> constexpr bool tma_in_place() { return AXIS != 2 && ((QUASI_TMA_INPLACE >> AXIS) & 1); }
 
 template <int AXIS, int P>
 __device__ __forceinline__ void tile_origin(const Geom& g, int tile, int& c0, int& c1, int& c2) {
@@ -483,7 +485,7 @@ inline TmaConfig& tma_config() {
   return c;
 }
 
-template <typename T, int N, int AXIS, int P, class Store, class Mul = NoMul, bool IP = kTmaInPlace && AXIS != 2>
+template <typename T, int N, int AXIS, int P, class Store, class Mul = NoMul, bool IP = tma_in_place<AXIS>()>
 cudaError_t launch_tma_pass(const Geom& g, int kind, Tables<T> tb, const T* src, Store st, cudaStream_t s,
                             Mul mul = Mul(), int dc1 = 0, int dc2 = 0, int ks = 0) {
   uint32_t box[3];
