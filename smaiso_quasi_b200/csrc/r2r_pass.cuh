@@ -336,11 +336,16 @@ template <typename T, int N, int AXIS, int P, bool IP> constexpr int tma_work_el
 }
 template <bool IP> constexpr int tma_min_blocks() { return IP ? 3 : 2; }
 
-template <typename T, int N, int AXIS, int P, class Store, class Mul, bool IP = false>
+// Mul2 != NoMul (x / y, not IP): each tile, loaded once, is transformed twice,
+// with mul into st and with mul2 into st2 (two inverse transforms of the same
+// spectral field that differ only in their multiplier).
+template <typename T, int N, int AXIS, int P, class Store, class Mul, bool IP = false, class Mul2 = NoMul>
 __global__ void __launch_bounds__(tma_threads<T>(), tma_min_blocks<IP>())
     tma_pass_kernel(const __grid_constant__ CUtensorMap map, Geom g, int kind, Tables<T> tb, Store st, int ntiles,
-                    int* err, Mul mul, int dc1, int dc2, int ks) {
+                    int* err, Mul mul, int dc1, int dc2, int ks, Store st2, Mul2 mul2) {
   static_assert(!IP || AXIS != 2, "in-place raw tiles are for x / y passes");
+  constexpr bool kDual = !std::is_same<Mul2, NoMul>::value;
+  static_assert(!kDual || (!IP && AXIS != 2), "dual tiles are x / y passes with a work tile");
   constexpr int NT = tma_threads<T>();
   constexpr int LD = tile_ld(N);
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -390,6 +395,16 @@ __global__ void __launch_bounds__(tma_threads<T>(), tma_min_blocks<IP>())
       __syncthreads();            // the last read of this raw buffer is done
       issue_next();
       continue;
+    } else if constexpr (AXIS != 2 && kDual) {
+      const int kt = g.nz / P;
+      const int outer = t / kt, k0 = (t - outer * kt) * P;
+      r2r_tile<T, N, P / 2, NT, false>(ex, tid, kind, reinterpret_cast<Cx<T>*>(work),
+                                        MulSrc<T, AXIS, Mul>{raw, P, outer, k0, mul},
+                                        GlobSnk<T, AXIS, Store>{st, outer, k0}, tb);
+      __syncthreads();   // the second transform rewrites the work tile
+      r2r_tile<T, N, P / 2, NT, false>(ex, tid, kind, reinterpret_cast<Cx<T>*>(work),
+                                        MulSrc<T, AXIS, Mul2>{raw, P, outer, k0, mul2},
+                                        GlobSnk<T, AXIS, Store>{st2, outer, k0}, tb, issue_next);
     } else if constexpr (AXIS != 2) {
       const int kt = g.nz / P;
       const int outer = t / kt, k0 = (t - outer * kt) * P;
@@ -485,9 +500,11 @@ inline TmaConfig& tma_config() {
   return c;
 }
 
-template <typename T, int N, int AXIS, int P, class Store, class Mul = NoMul, bool IP = tma_in_place<AXIS>()>
+template <typename T, int N, int AXIS, int P, class Store, class Mul = NoMul, class Mul2 = NoMul,
+          bool IP = tma_in_place<AXIS>() && std::is_same<Mul2, NoMul>::value>
 cudaError_t launch_tma_pass(const Geom& g, int kind, Tables<T> tb, const T* src, Store st, cudaStream_t s,
-                            Mul mul = Mul(), int dc1 = 0, int dc2 = 0, int ks = 0) {
+                            Mul mul = Mul(), int dc1 = 0, int dc2 = 0, int ks = 0, Store st2 = Store(),
+                            Mul2 mul2 = Mul2()) {
   uint32_t box[3];
   constexpr int SUB = (N + 255) / 256;
   if (AXIS == 2) { box[0] = N; box[1] = P; box[2] = 1; }
@@ -496,7 +513,7 @@ cudaError_t launch_tma_pass(const Geom& g, int kind, Tables<T> tb, const T* src,
   CUtensorMap map;
   if (!MapCache::get().lookup(&map, src, int(sizeof(T)), g.nx, g.ny, g.nz, AXIS, box)) return cudaErrorNotSupported;
   const size_t smem = tma_smem_bytes<T, N, AXIS, P, IP>();
-  auto kern = tma_pass_kernel<T, N, AXIS, P, Store, Mul, IP>;
+  auto kern = tma_pass_kernel<T, N, AXIS, P, Store, Mul, IP, Mul2>;
   static int per_sm = 0;   // per instantiation: resident CTAs per SM
   if (per_sm == 0) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -511,7 +528,8 @@ cudaError_t launch_tma_pass(const Geom& g, int kind, Tables<T> tb, const T* src,
   else if (AXIS == 1) tiles = g.nx * (g.nz / P);
   else tiles = g.ny * (g.nz / P);
   const int grid = tiles < per_sm * tma_config().sms ? tiles : per_sm * tma_config().sms;
-  kern<<<grid, tma_threads<T>(), smem, s>>>(map, g, kind, tb, st, tiles, tma_config().err, mul, dc1, dc2, ks);
+  kern<<<grid, tma_threads<T>(), smem, s>>>(map, g, kind, tb, st, tiles, tma_config().err, mul, dc1, dc2, ks, st2,
+                                             mul2);
   return cudaGetLastError();
 }
 
@@ -625,6 +643,39 @@ cudaError_t launch_mul_x_pass(const Geom& g, int kind, Tables<T> tb, const T* sr
 #undef QUASI_TMA_CASE
   }
   return launch_pass<T, 0>(g, kind, tb, MulLoad<T, Mul>{g, src, mul, di, dj}, st, s);
+}
+
+// Two x passes of the same shifted source with different multipliers, one tile
+// load each (the general kernel runs them one after the other).
+template <typename T, class Mul, class Mul2, class Store>
+cudaError_t launch_mul_x_pass2(const Geom& g, int kind, Tables<T> tb, const T* src, Mul mul, Mul2 mul2, int di, int dj,
+                               Store st, Store st2, cudaStream_t s) {
+  const long extent = g.nz;
+  if (tma_config().enabled && tma_config().err) {
+#define QUASI_TMA_CASE(NN)                                                                              \
+    case NN: {                                                                                          \
+      constexpr int P = pass_pencils<T>(NN);                                                            \
+      if (extent % P == 0)                                                                              \
+        return launch_tma_pass<T, NN, 0, P, Store, Mul, Mul2>(g, kind, tb, src, st, s, mul, dj, di, 0, st2, \
+                                                              mul2);                                    \
+      break;                                                                                            \
+    }
+    switch (g.nx) {
+      QUASI_TMA_CASE(16)
+      QUASI_TMA_CASE(32)
+      QUASI_TMA_CASE(64)
+      QUASI_TMA_CASE(96)
+      QUASI_TMA_CASE(128)
+      QUASI_TMA_CASE(192)
+      QUASI_TMA_CASE(256)
+      QUASI_TMA_CASE(512)
+      default: break;
+    }
+#undef QUASI_TMA_CASE
+  }
+  cudaError_t e = launch_pass<T, 0>(g, kind, tb, MulLoad<T, Mul>{g, src, mul, di, dj}, st, s);
+  if (e != cudaSuccess) return e;
+  return launch_pass<T, 0>(g, kind, tb, MulLoad<T, Mul2>{g, src, mul2, di, dj}, st2, s);
 }
 
 }  // namespace quasi

@@ -562,6 +562,19 @@ cudaError_t forward3(const Geom& g, const AxisTables<T>& tb, const int kinds[3],
   return launch_pass<T, 0>(g, kinds[0], tb.t[0], LoadField<T>{g, dst}, st, s);
 }
 
+// Two inverses of the same spectral source that differ only in their
+// multiplier (same kinds and shifts): one dual x pass, then y and z of each.
+template <typename T, class Mul, class Mul2>
+cudaError_t inverse3_mul2(const Geom& g, const AxisTables<T>& tb, const int kinds[3], const T* src, Mul mul, Mul2 mul2,
+                          int di, int dj, int dk, T* dst, T* dst2, cudaStream_t s) {
+  cudaError_t e;
+  if ((e = launch_mul_x_pass2<T>(g, kinds[0], tb.t[0], src, mul, mul2, di, dj, StoreField<T>{g, dst},
+                                 StoreField<T>{g, dst2}, s)) != cudaSuccess)
+    return e;
+  if ((e = yz3(g, tb, kinds, dst, StoreField<T>{g, dst}, s, dk)) != cudaSuccess) return e;
+  return yz3(g, tb, kinds, dst2, StoreField<T>{g, dst2}, s, dk);
+}
+
 // FFTW kinds per plan (quasi.cpp:449-495), axes (x, y, z)
 constexpr int kCT[3] = {E10, E10, E10};
 constexpr int kiCT[3] = {E01, E01, E01};
@@ -612,18 +625,15 @@ cudaError_t enqueue_step(const StepCtx<T>& c, const AxisTables<T>& tb, int* nloo
   auto ld = [&](T* d) { return LoadField<T>{g, d}; };
   if (c.variant == kQuasi) {
     // a3 prologue quasi.cpp:1036-1057
-    QUASI_TRY(inverse3_mul(g, tb, kiCT, c.psiq, MDf<T>{c}, 0, 0, 0, st(c.df), c.df, s));
-    QUASI_TRY(inverse3_mul(g, tb, kiCT, c.psiq, MLap<T>{c}, 0, 0, 0, st(c.lap), c.lap, s));
-    // a4 gradients quasi.cpp:1120-1232
-    QUASI_TRY(inverse3_mul(g, tb, kiSTx, c.psiq, MGrad<T, 0, false>{c}, 1, 0, 0, st(c.gx), c.gx, s));
-    QUASI_TRY(inverse3_mul(g, tb, kiSTy, c.psiq, MGrad<T, 1, false>{c}, 0, 1, 0, st(c.gy), c.gy, s));
-    QUASI_TRY(inverse3_mul(g, tb, kiSTz, c.psiq, MGrad<T, 2, false>{c}, 0, 0, 1, st(c.gz), c.gz, s));
+    // (pairs that share the source, kinds and shift take one dual x pass)
+    QUASI_TRY(inverse3_mul2(g, tb, kiCT, c.psiq, MDf<T>{c}, MLap<T>{c}, 0, 0, 0, c.df, c.lap, s));
+    // a4 gradients quasi.cpp:1120-1232: grad psi with grad lap grad psi, grad rho
+    QUASI_TRY(inverse3_mul2(g, tb, kiSTx, c.psiq, MGrad<T, 0, false>{c}, MGrad<T, 0, true>{c}, 1, 0, 0, c.gx, c.ldx, s));
+    QUASI_TRY(inverse3_mul2(g, tb, kiSTy, c.psiq, MGrad<T, 1, false>{c}, MGrad<T, 1, true>{c}, 0, 1, 0, c.gy, c.ldy, s));
+    QUASI_TRY(inverse3_mul2(g, tb, kiSTz, c.psiq, MGrad<T, 2, false>{c}, MGrad<T, 2, true>{c}, 0, 0, 1, c.gz, c.ldz, s));
     QUASI_TRY(inverse3_mul(g, tb, kiSTx, c.rhoq, MGrad<T, 0, false>{c}, 1, 0, 0, st(c.rdx), c.rdx, s));
     QUASI_TRY(inverse3_mul(g, tb, kiSTy, c.rhoq, MGrad<T, 1, false>{c}, 0, 1, 0, st(c.rdy), c.rdy, s));
     QUASI_TRY(inverse3_mul(g, tb, kiSTz, c.rhoq, MGrad<T, 2, false>{c}, 0, 0, 1, st(c.rdz), c.rdz, s));
-    QUASI_TRY(inverse3_mul(g, tb, kiSTx, c.psiq, MGrad<T, 0, true>{c}, 1, 0, 0, st(c.ldx), c.ldx, s));
-    QUASI_TRY(inverse3_mul(g, tb, kiSTy, c.psiq, MGrad<T, 1, true>{c}, 0, 1, 0, st(c.ldy), c.ldy, s));
-    QUASI_TRY(inverse3_mul(g, tb, kiSTz, c.psiq, MGrad<T, 2, true>{c}, 0, 0, 1, st(c.ldz), c.ldz, s));
     // a5 density + filter quasi.cpp:1237-1268 (rho doubles as the scratch)
     QUASI_EW(rho_law_kernel<T>, c, n);
     QUASI_TRY(cudaGetLastError());

@@ -49,14 +49,24 @@ struct ZTile {
     int ks;
     QHD T at(int r, int n) const { return n + ks < N ? raw[r * N + n + ks] : T(0); }
   };
-  QHD static Cx<T> fwd_in(const Rows& src, int kind, int g, int e) {
+  // the same with the shift fixed at compile time (the kernel's form)
+  template <int KS> struct RowsK {
+    const T* raw;
+    QHD T at(int r, int n) const {
+      if constexpr (KS == 0) return raw[r * N + n];
+      else return n + KS < N ? raw[r * N + n + KS] : T(0);
+    }
+  };
+  template <class Src>
+  QHD static Cx<T> fwd_in(const Src& src, int kind, int g, int e) {
     int n;
     T sgn = T(1);
     if (e < N / 2) n = 2 * e;
     else { n = 2 * (N - 1 - e) + 1; if (kind == O10) sgn = T(-1); }
     return Cx<T>{sgn * src.at(2 * g, n), sgn * src.at(2 * g + 1, n)};
   }
-  QHD static Cx<T> inv_in(const Rows& src, int kind, int g, int k, Tables<T> tb) {
+  template <class Src>
+  QHD static Cx<T> inv_in(const Src& src, int kind, int g, int k, Tables<T> tb) {
     const bool rev = kind == O01;
     const int n0 = rev ? N - 1 - k : k;
     const T ak = src.at(2 * g, n0), bk = src.at(2 * g + 1, n0);
@@ -74,7 +84,8 @@ struct ZTile {
   }
 
   // first stage read (s = 1): butterfly b of pencil g takes e = b + t N/R
-  QHD static void first_read(int tid, const Rows& src, int kind, Tables<T> tb, Regs<R1>& r) {
+  template <class Src>
+  QHD static void first_read(int tid, const Src& src, int kind, Tables<T> tb, Regs<R1>& r) {
     constexpr int R = R1, M = N / R;
 #pragma unroll
     for (int c = 0; c < per_thread<R>(); ++c) {
@@ -319,10 +330,10 @@ __device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_
 // TMA store.  One thread issues all copies; the landing buffer of tile t is
 // refilled (tile t + 2 gridDim.x) as soon as the first stage has read it, and
 // the staging rows are rewritten only after the previous store has read them.
-template <typename T, int N, int P>
+template <typename T, int N, int P, int KS>
 __global__ void __launch_bounds__(256, 2)
     tma_zpass_kernel(const __grid_constant__ CUtensorMap src_map, const __grid_constant__ CUtensorMap dst_map, Geom g,
-                     int kind, Tables<T> tb, int ntiles, int* err, int ks) {
+                     int kind, Tables<T> tb, int ntiles, int* err) {
   constexpr int NT = 256, G = P / 2;
   using Z = ZTile<T, N, G, NT>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -366,7 +377,7 @@ __global__ void __launch_bounds__(256, 2)
     }
     // first stage: dense rows -> registers | previous store read out | -> padded tile
     typename Z::template Regs<Z::R1> r1;
-    Z::first_read(tid, typename Z::Rows{raw, ks}, kind, tb, r1);
+    Z::first_read(tid, typename Z::template RowsK<KS>{raw}, kind, tb, r1);
     if (tid == 0) bulk_wait_read0();
     __syncthreads();
     if (tid == 0 && t + 2 * int(gridDim.x) < ntiles) {
@@ -393,8 +404,8 @@ __global__ void __launch_bounds__(256, 2)
 #define QUASI_ZPASS 1
 #endif
 
-template <typename T, int N>
-cudaError_t launch_zpass_n(const Geom& g, int kind, Tables<T> tb, const T* src, T* dst, cudaStream_t s, int ks) {
+template <typename T, int N, int KS>
+cudaError_t launch_zpass_nk(const Geom& g, int kind, Tables<T> tb, const T* src, T* dst, cudaStream_t s) {
   constexpr int P = pass_pencils<T>(N), G = P / 2;
   using Z = ZTile<T, N, G, 256>;
   if (g.ny % P != 0) return cudaErrorNotSupported;
@@ -404,7 +415,7 @@ cudaError_t launch_zpass_n(const Geom& g, int kind, Tables<T> tb, const T* src, 
       !MapCache::get().lookup(&dmap, dst, int(sizeof(T)), g.nx, g.ny, g.nz, 2, box))
     return cudaErrorNotSupported;
   const size_t smem = size_t(2) * P * N * sizeof(T) + ((Z::cb_bytes() + 15) / 16) * 16 + 16;
-  auto kern = tma_zpass_kernel<T, N, P>;
+  auto kern = tma_zpass_kernel<T, N, P, KS>;
   static int per_sm = 0;   // per instantiation
   if (per_sm == 0) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
@@ -416,8 +427,13 @@ cudaError_t launch_zpass_n(const Geom& g, int kind, Tables<T> tb, const T* src, 
   }
   const int tiles = (g.nx * g.ny) / P;
   const int grid = tiles < per_sm * tma_config().sms ? tiles : per_sm * tma_config().sms;
-  kern<<<grid, 256, smem, s>>>(smap, dmap, g, kind, tb, tiles, tma_config().err, ks);
+  kern<<<grid, 256, smem, s>>>(smap, dmap, g, kind, tb, tiles, tma_config().err);
   return cudaGetLastError();
+}
+
+template <typename T, int N>
+cudaError_t launch_zpass_n(const Geom& g, int kind, Tables<T> tb, const T* src, T* dst, cudaStream_t s, int ks) {
+  return ks ? launch_zpass_nk<T, N, 1>(g, kind, tb, src, dst, s) : launch_zpass_nk<T, N, 0>(g, kind, tb, src, dst, s);
 }
 
 // z pass src -> dst (plain fields; ks = 1 transforms row[k + 1], zero at the
