@@ -84,8 +84,11 @@ struct ZTile {
   }
 
   // first stage read (s = 1): butterfly b of pencil g takes e = b + t N/R
+  // tw1 (optional): the first stage's twiddles W_N^{b u} as tw1[u * (N/R1) + b]
+  // (a warp reads consecutive entries); otherwise tb.root[b u]
   template <class Src>
-  QHD static void first_read(int tid, const Src& src, int kind, Tables<T> tb, Regs<R1>& r) {
+  QHD static void first_read(int tid, const Src& src, int kind, Tables<T> tb, Regs<R1>& r,
+                             const Cx<T>* tw1 = nullptr) {
     constexpr int R = R1, M = N / R;
 #pragma unroll
     for (int c = 0; c < per_thread<R>(); ++c) {
@@ -115,7 +118,7 @@ struct ZTile {
       Dft<T, R>::run(r.v[c]);
 #pragma unroll
       for (int u = 1; u < R; ++u)
-        if (b) r.v[c][u] = cmul(r.v[c][u], tb.root[b * u]);
+        if (b) r.v[c][u] = cmul(r.v[c][u], tw1 ? tw1[u * M + b] : tb.root[b * u]);
     }
   }
 
@@ -342,7 +345,20 @@ __global__ void __launch_bounds__(256, 2)
   Cx<T>* cb = reinterpret_cast<Cx<T>*>(raw1 + P * N);
   T* stg = reinterpret_cast<T*>(cb);
   uint64_t* bar = reinterpret_cast<uint64_t*>(reinterpret_cast<unsigned char*>(cb) + ((Z::cb_bytes() + 15) / 16) * 16);
+  // per-CTA copies of the twiddles: stage 1's as [u][b], and the quarter-wave
+  // table the pre-twiddle and the unpack read
+  Cx<T>* tw1 = reinterpret_cast<Cx<T>*>(bar + 2);
+  Cx<T>* qt = tw1 + N;
   const int tid = threadIdx.x;
+  {
+    constexpr int M = N / Z::R1;
+    for (int e = tid; e < N; e += 256) {
+      const int u = e / M, b = e - u * M;
+      tw1[e] = tb.root[b * u];
+      qt[e] = tb.quarter[e];
+    }
+    tb.quarter = qt;
+  }
   auto origin = [&](int t, int& c1, int& c2) {
     const int row = t * P;
     c2 = row / g.ny;
@@ -377,7 +393,7 @@ __global__ void __launch_bounds__(256, 2)
     }
     // first stage: dense rows -> registers | previous store read out | -> padded tile
     typename Z::template Regs<Z::R1> r1;
-    Z::first_read(tid, typename Z::template RowsK<KS>{raw}, kind, tb, r1);
+    Z::first_read(tid, typename Z::template RowsK<KS>{raw}, kind, tb, r1, tw1);
     if (tid == 0) bulk_wait_read0();
     __syncthreads();
     if (tid == 0 && t + 2 * int(gridDim.x) < ntiles) {
@@ -414,7 +430,7 @@ cudaError_t launch_zpass_nk(const Geom& g, int kind, Tables<T> tb, const T* src,
   if (!MapCache::get().lookup(&smap, src, int(sizeof(T)), g.nx, g.ny, g.nz, 2, box) ||
       !MapCache::get().lookup(&dmap, dst, int(sizeof(T)), g.nx, g.ny, g.nz, 2, box))
     return cudaErrorNotSupported;
-  const size_t smem = size_t(2) * P * N * sizeof(T) + ((Z::cb_bytes() + 15) / 16) * 16 + 16;
+  const size_t smem = size_t(2) * P * N * sizeof(T) + ((Z::cb_bytes() + 15) / 16) * 16 + 16 + 2 * N * sizeof(Cx<T>);
   auto kern = tma_zpass_kernel<T, N, P, KS>;
   static int per_sm = 0;   // per instantiation
   if (per_sm == 0) {
