@@ -354,6 +354,17 @@ __global__ void __launch_bounds__(tma_threads<T>(), tma_min_blocks<IP>())
   T* work = raw1 + P * N;
   uint64_t* bar = reinterpret_cast<uint64_t*>(work + tma_work_elems<T, N, AXIS, P, IP>());
   const int tid = threadIdx.x;
+  {
+    // per-CTA shared-memory copies of the twiddle tables (N entries each)
+    Cx<T>* rt = reinterpret_cast<Cx<T>*>(bar + 2);
+    Cx<T>* qt = rt + N;
+    for (int e = tid; e < N; e += NT) {
+      rt[e] = tb.root[e];
+      qt[e] = tb.quarter[e];
+    }
+    tb.root = rt;
+    tb.quarter = qt;
+  }
   if (tid == 0) {
     mbar_init(&bar[0], 1);
     mbar_init(&bar[1], 1);
@@ -456,7 +467,8 @@ __global__ void __launch_bounds__(tma_threads<T>(), tma_min_blocks<IP>())
 
 template <typename T, int N, int AXIS, int P, bool IP>
 inline size_t tma_smem_bytes() {
-  return size_t(2) * P * N * sizeof(T) + size_t(tma_work_elems<T, N, AXIS, P, IP>()) * sizeof(T) + 64;
+  return size_t(2) * P * N * sizeof(T) + size_t(tma_work_elems<T, N, AXIS, P, IP>()) * sizeof(T) + 16 +
+         2 * N * sizeof(Cx<T>);
 }
 
 // Pencils per tile.  z: rows per CTA; x/y: consecutive k (coalescing width).
