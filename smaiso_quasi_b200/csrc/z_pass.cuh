@@ -32,9 +32,11 @@ struct ZTile {
   static_assert(plan.n_stages > 0, "unsupported transform length");
   static constexpr int R1 = plan.r[0];
   QHD static constexpr int phi(int e) { return e + e / R1; }
-  // padded pencil stride (complex), rounded to 8 mod 16 so that pencils
-  // sharing a warp start on different bank halves
-  static constexpr int LDC = ((phi(N - 1) + 1 + 7) / 16) * 16 + 8;
+  // padded pencil stride (complex).  FP32: rounded to 8 mod 16 so that two
+  // pencils sharing a warp start on different bank halves; FP64 (a warp
+  // never spans two pencils of the sizes that matter) just even
+  static constexpr int LDC =
+      sizeof(T) == 8 ? ((phi(N - 1) + 2) / 2) * 2 : ((phi(N - 1) + 1 + 7) / 16) * 16 + 8;
   static constexpr size_t cb_bytes() { return size_t(G) * LDC * sizeof(Cx<T>); }
   static_assert(LDC >= N, "the staging rows overlay the padded tile");
 
@@ -349,6 +351,7 @@ __global__ void __launch_bounds__(256, 2)
   // table the pre-twiddle and the unpack read
   Cx<T>* tw1 = reinterpret_cast<Cx<T>*>(bar + 2);
   Cx<T>* qt = tw1 + N;
+  Cx<T>* rt = qt + N;   // the root table itself, for the later stages
   const int tid = threadIdx.x;
   {
     constexpr int M = N / Z::R1;
@@ -356,8 +359,10 @@ __global__ void __launch_bounds__(256, 2)
       const int u = e / M, b = e - u * M;
       tw1[e] = tb.root[b * u];
       qt[e] = tb.quarter[e];
+      rt[e] = tb.root[e];
     }
     tb.quarter = qt;
+    tb.root = rt;
   }
   auto origin = [&](int t, int& c1, int& c2) {
     const int row = t * P;
@@ -430,7 +435,7 @@ cudaError_t launch_zpass_nk(const Geom& g, int kind, Tables<T> tb, const T* src,
   if (!MapCache::get().lookup(&smap, src, int(sizeof(T)), g.nx, g.ny, g.nz, 2, box) ||
       !MapCache::get().lookup(&dmap, dst, int(sizeof(T)), g.nx, g.ny, g.nz, 2, box))
     return cudaErrorNotSupported;
-  const size_t smem = size_t(2) * P * N * sizeof(T) + ((Z::cb_bytes() + 15) / 16) * 16 + 16 + 2 * N * sizeof(Cx<T>);
+  const size_t smem = size_t(2) * P * N * sizeof(T) + ((Z::cb_bytes() + 15) / 16) * 16 + 16 + 3 * N * sizeof(Cx<T>);
   auto kern = tma_zpass_kernel<T, N, P, KS>;
   static int per_sm = 0;   // per instantiation
   if (per_sm == 0) {
