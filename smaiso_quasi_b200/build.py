@@ -69,7 +69,7 @@ def build(verbose: bool = False, jobs: int | None = None, ptxas_info: bool = Fal
     with cf.ThreadPoolExecutor(max_workers=jobs or min(8, os.cpu_count() or 4)) as ex:
         list(ex.map(_run, todo))
     if todo or not LIB.exists():
-        _run([cc, *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lcudart"])
+        _run([cc, *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lcudart", "-lpthread"])
     drv_src = CSRC / "quasi_run.cpp"
     if drv_src.exists() and _stale(DRIVER, [drv_src, LIB] + hdrs):
         _run(["g++", "-O2", "-std=c++17", "-I", str(ROOT / "include"), str(drv_src), "-o", str(DRIVER),

@@ -3,11 +3,13 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/quasi_gpu.h"
@@ -36,6 +38,26 @@ class EngineBase {
 
 EngineBase* make_engine_f64(const quasi_config& cfg, std::string& err);
 EngineBase* make_engine_f32(const quasi_config& cfg, std::string& err);
+
+// Host loop over [0, n) split into contiguous chunks on up to 16 threads (the
+// field conversions between the caller's doubles and the staging buffer).
+template <class F>
+inline void host_parallel(size_t n, F&& f) {
+  unsigned hw = std::thread::hardware_concurrency();
+  const size_t nt = std::min<size_t>(hw ? hw : 1, 16);
+  if (nt <= 1 || n < (size_t(1) << 20)) {
+    f(size_t(0), n);
+    return;
+  }
+  std::vector<std::thread> pool;
+  const size_t chunk = (n + nt - 1) / nt;
+  for (size_t t = 1; t < nt; ++t) {
+    const size_t lo = std::min(n, t * chunk), hi = std::min(n, lo + chunk);
+    pool.emplace_back([&f, lo, hi] { f(lo, hi); });
+  }
+  f(size_t(0), std::min(n, chunk));
+  for (auto& th : pool) th.join();
+}
 
 // QUASI_FUSED_YZ=1 selects the one-pass y+z cluster kernel (yz_plane.cuh)
 // for the plane shapes it covers; by default the y and z passes run as two

@@ -125,13 +125,17 @@ class Engine : public EngineBase {
       if (!cuda_ok(tw_[a].upload(len[a]), "twiddles")) return QUASI_ERR_CUDA;
     for (int a = 0; a < 3; ++a) tb_.t[a] = tw_[a].tables();
     build_ctx(h);
-    return QUASI_OK;
+    // the six step graphs are made here, like the reference's FFTW plans
+    // before its loop: quasi_step only launches them
+    return capture();
   }
 
   int set_psi(const double* host) override {
     set_phase(0);   // quasi_init starts the rotation at phase 0
     T* st = static_cast<T*>(host_stage_);
-    for (size_t i = 0; i < n_; ++i) st[i] = T(host[i]);
+    host_parallel(n_, [&](size_t lo, size_t hi) {
+      for (size_t i = lo; i < hi; ++i) st[i] = T(host[i]);
+    });
     if (!cuda_ok(cudaMemcpyAsync(c_.psi, st, n_ * sizeof(T), cudaMemcpyHostToDevice, stream_), "H2D")) return QUASI_ERR_CUDA;
     if (!cuda_ok(cudaStreamSynchronize(stream_), "sync")) return QUASI_ERR_CUDA;
     have_psi_ = true;
@@ -180,7 +184,9 @@ class Engine : public EngineBase {
     T* st = static_cast<T*>(host_stage_);
     if (!cuda_ok(cudaMemcpyAsync(st, src, n_ * sizeof(T), cudaMemcpyDeviceToHost, stream_), "D2H")) return QUASI_ERR_CUDA;
     if (!cuda_ok(cudaStreamSynchronize(stream_), "sync")) return QUASI_ERR_CUDA;
-    for (size_t i = 0; i < n_; ++i) host[i] = double(st[i]);
+    host_parallel(n_, [&](size_t lo, size_t hi) {
+      for (size_t i = lo; i < hi; ++i) host[i] = double(st[i]);
+    });
     return QUASI_OK;
   }
 
