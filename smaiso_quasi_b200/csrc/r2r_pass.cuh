@@ -275,9 +275,11 @@ struct MulSrc {
     if constexpr (Mul::kActive) {
       const int k = k0 + 2 * g;
       const int i = AXIS == 1 ? outer : n, j = AXIS == 1 ? n : outer;
-      using M = decltype(mul(i, j, k));   // the multiplier's own type
-      a = T(M(a) * mul(i, j, k));
-      b = T(M(b) * mul(i, j, k + 1));
+      // the multiplier is evaluated in its own type (double where q0^2 - q^2
+      // cancels), rounded to the storage type once, and applied there: one
+      // conversion per element instead of two
+      a *= T(mul(i, j, k));
+      b *= T(mul(i, j, k + 1));
     }
   }
 };
