@@ -47,7 +47,8 @@ __device__ __forceinline__ double sq(double x) { return x * x; }
 // semi-implicit update and the reductions always use double.
 template <typename T> using Arith = T;
 __device__ __forceinline__ double rcp(double x) { return __drcp_rn(x); }
-__device__ __forceinline__ float rcp(float x) { return __frcp_rn(x); }
+// FP32: the hardware reciprocal (within 2 ulp, below the FP32 storage rounding)
+__device__ __forceinline__ float rcp(float x) { return __fdividef(1.0f, x); }
 
 template <typename T>
 __device__ __forceinline__ size_t at(const StepCtx<T>& c, int i, int j, int k) { return lin(c.g, i, j, k); }
@@ -279,7 +280,7 @@ __device__ __forceinline__ void shift_next(const Pack<T>& a, const T* row_ptr, i
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) project_kernel(StepCtx<T> c) {
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) project_kernel(StepCtx<T> c) {
   using A = Arith<T>;
   constexpr int V = Pack<T>::V;
   const Geom g = c.g;
