@@ -260,6 +260,9 @@ struct NoMul {
   __device__ double operator()(int, int, int) const { return 1.0; }
 };
 
+template <class M, class = void> struct MulCol { struct type {}; };
+template <class M> struct MulCol<M, std::void_t<typename M::Col>> { using type = typename M::Col; };
+
 // x / y tile source with a per-element multiplier of the OUTPUT index
 // (i, j, k): the spectral prologue of an inverse transform.
 template <typename T, int AXIS, class Mul, bool ALIAS = false>
@@ -268,18 +271,31 @@ struct MulSrc {
   const T* raw;
   int P, outer, k0;
   Mul mul;
+  // x passes: the column parts of this thread's two pencils (prep)
+  typename MulCol<Mul>::type ca{}, cb{};
+  // gt = the one pencil pair this thread reads: the first stage's pencil-fastest
+  // mapping gives g = tid % (P/2) whenever the thread count is a multiple of P/2
+  __device__ void prep(int gt) {
+    if constexpr (Mul::kActive && AXIS == 0) {
+      ca = mul.col(outer, k0 + 2 * gt);
+      cb = mul.col(outer, k0 + 2 * gt + 1);
+    }
+  }
   QHD void pair(int g, int n, T& a, T& b) const {
     const typename Vec2<T>::type v = *reinterpret_cast<const typename Vec2<T>::type*>(raw + n * P + 2 * g);
     a = v.x;
     b = v.y;
     if constexpr (Mul::kActive) {
-      const int k = k0 + 2 * g;
-      const int i = AXIS == 1 ? outer : n, j = AXIS == 1 ? n : outer;
       // the multiplier is evaluated in its own type (double where q0^2 - q^2
-      // cancels), rounded to the storage type once, and applied there: one
-      // conversion per element instead of two
-      a *= T(mul(i, j, k));
-      b *= T(mul(i, j, k + 1));
+      // cancels), rounded to the storage type once, and applied there
+      if constexpr (AXIS == 0) {
+        a *= T(mul.row(n, ca));
+        b *= T(mul.row(n, cb));
+      } else {
+        const int k = k0 + 2 * g;
+        a *= T(mul(outer, n, k));
+        b *= T(mul(outer, n, k + 1));
+      }
     }
   }
 };
@@ -347,6 +363,7 @@ __global__ void __launch_bounds__(tma_threads<T>(), tma_min_blocks<IP>())
                     int* err, Mul mul, int dc1, int dc2, int ks, Store st2, Mul2 mul2) {
   static_assert(!IP || AXIS != 2, "in-place raw tiles are for x / y passes");
   constexpr bool kDual = !std::is_same<Mul2, NoMul>::value;
+  static_assert(tma_threads<T>() % (P / 2) == 0, "MulSrc::prep: each thread reads one pencil pair");
   static_assert(!kDual || (!IP && AXIS != 2), "dual tiles are x / y passes with a work tile");
   constexpr int NT = tma_threads<T>();
   constexpr int LD = tile_ld(N);
@@ -401,8 +418,9 @@ __global__ void __launch_bounds__(tma_threads<T>(), tma_min_blocks<IP>())
     if constexpr (AXIS != 2 && IP) {
       const int kt = g.nz / P;
       const int outer = t / kt, k0 = (t - outer * kt) * P;
-      r2r_tile<T, N, P / 2, NT, false, ElemMajor<P / 2>>(ex, tid, kind, reinterpret_cast<Cx<T>*>(raw),
-                                                          MulSrc<T, AXIS, Mul, true>{raw, P, outer, k0, mul},
+      MulSrc<T, AXIS, Mul, true> src{raw, P, outer, k0, mul};
+      src.prep(tid % (P / 2));
+      r2r_tile<T, N, P / 2, NT, false, ElemMajor<P / 2>>(ex, tid, kind, reinterpret_cast<Cx<T>*>(raw), src,
                                                           GlobSnk<T, AXIS, Store>{st, outer, k0}, tb);
       fence_proxy_async_smem();   // this thread's writes to raw precede the copy that refills it
       __syncthreads();            // the last read of this raw buffer is done
@@ -411,18 +429,21 @@ __global__ void __launch_bounds__(tma_threads<T>(), tma_min_blocks<IP>())
     } else if constexpr (AXIS != 2 && kDual) {
       const int kt = g.nz / P;
       const int outer = t / kt, k0 = (t - outer * kt) * P;
-      r2r_tile<T, N, P / 2, NT, false>(ex, tid, kind, reinterpret_cast<Cx<T>*>(work),
-                                        MulSrc<T, AXIS, Mul>{raw, P, outer, k0, mul},
+      MulSrc<T, AXIS, Mul> src{raw, P, outer, k0, mul};
+      src.prep(tid % (P / 2));
+      r2r_tile<T, N, P / 2, NT, false>(ex, tid, kind, reinterpret_cast<Cx<T>*>(work), src,
                                         GlobSnk<T, AXIS, Store>{st, outer, k0}, tb);
       __syncthreads();   // the second transform rewrites the work tile
-      r2r_tile<T, N, P / 2, NT, false>(ex, tid, kind, reinterpret_cast<Cx<T>*>(work),
-                                        MulSrc<T, AXIS, Mul2>{raw, P, outer, k0, mul2},
+      MulSrc<T, AXIS, Mul2> src2{raw, P, outer, k0, mul2};
+      src2.prep(tid % (P / 2));
+      r2r_tile<T, N, P / 2, NT, false>(ex, tid, kind, reinterpret_cast<Cx<T>*>(work), src2,
                                         GlobSnk<T, AXIS, Store>{st2, outer, k0}, tb, issue_next);
     } else if constexpr (AXIS != 2) {
       const int kt = g.nz / P;
       const int outer = t / kt, k0 = (t - outer * kt) * P;
-      r2r_tile<T, N, P / 2, NT, false>(ex, tid, kind, reinterpret_cast<Cx<T>*>(work),
-                                        MulSrc<T, AXIS, Mul>{raw, P, outer, k0, mul},
+      MulSrc<T, AXIS, Mul> src{raw, P, outer, k0, mul};
+      src.prep(tid % (P / 2));
+      r2r_tile<T, N, P / 2, NT, false>(ex, tid, kind, reinterpret_cast<Cx<T>*>(work), src,
                                         GlobSnk<T, AXIS, Store>{st, outer, k0}, tb, issue_next);
     } else {
       // dense rows -> padded in-place tile (both sides contiguous in n); ks = 1

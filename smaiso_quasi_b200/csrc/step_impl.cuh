@@ -63,48 +63,72 @@ __device__ __forceinline__ double mq2c(const StepCtx<T>& c, int i, int j, int k)
 // inverse transforms, in double (the x pass rounds the product once).  The
 // spectrum concentrates on the ring |q| = q0, where q0^2 - q^2 cancels.
 // ---------------------------------------------------------------------------
-template <typename T>
-__device__ __forceinline__ double dq2(const StepCtx<T>& c, int i, int j, int k) {   // quasi.cpp:882
-  const double x = __ldg(c.vqx + i), y = __ldg(c.vqy + j), z = __ldg(c.vqz + k);
-  return x * x + y * y + z * z;
-}
+// Each multiplier splits into a column part (j, k: fixed for a thread of an
+// x-pass tile, computed once per tile) and a row part (i, per element):
+// row(i, col(j, k)) == operator()(i, j, k).
 template <typename T> struct MDf {      // dfDlapPsi, quasi.cpp:1044
   static constexpr bool kActive = true;
   StepCtx<T> c;
-  __device__ double operator()(int i, int j, int k) const { return c.alpha * (c.q0 * c.q0 - dq2(c, i, j, k)); }
+  struct Col { double s; };             // qy^2 + qz^2
+  __device__ Col col(int j, int k) const {
+    const double y = __ldg(c.vqy + j), z = __ldg(c.vqz + k);
+    return {y * y + z * z};
+  }
+  __device__ double q2(int i, const Col& cl) const {   // quasi.cpp:882
+    const double x = __ldg(c.vqx + i);
+    return x * x + cl.s;
+  }
+  __device__ double row(int i, const Col& cl) const { return c.alpha * (c.q0 * c.q0 - q2(i, cl)); }
+  __device__ double operator()(int i, int j, int k) const { return row(i, col(j, k)); }
 };
 template <typename T> struct MLap {     // lapRhoDfDlapPsi, quasi.cpp:1046-1047
   static constexpr bool kActive = true;
   StepCtx<T> c;
-  __device__ double operator()(int i, int j, int k) const {
-    const double q2 = dq2(c, i, j, k);
+  using Col = typename MDf<T>::Col;
+  __device__ Col col(int j, int k) const { return MDf<T>{c}.col(j, k); }
+  __device__ double row(int i, const Col& cl) const {
+    const double q2 = MDf<T>{c}.q2(i, cl);
     return -q2 * (c.alpha * (c.q0 * c.q0 - q2));
   }
+  __device__ double operator()(int i, int j, int k) const { return row(i, col(j, k)); }
 };
 template <typename T> struct MSh {      // -aLin, quasi-stb.cpp:1019
   static constexpr bool kActive = true;
   StepCtx<T> c;
-  __device__ double operator()(int i, int j, int k) const {
-    const double d = c.q0 * c.q0 - dq2(c, i, j, k);
+  using Col = typename MDf<T>::Col;
+  __device__ Col col(int j, int k) const { return MDf<T>{c}.col(j, k); }
+  __device__ double row(int i, const Col& cl) const {
+    const double d = c.q0 * c.q0 - MDf<T>{c}.q2(i, cl);
     return -(c.ep - c.alpha * (d * d));
   }
+  __device__ double operator()(int i, int j, int k) const { return row(i, col(j, k)); }
 };
 // Shifted gradient along A, quasi.cpp:1120-1186.  The input is read at
 // index + 1 along x or y by the TMA box offset (the row past the end reads as
 // zero: the reference's zero top DST index); along z the z pass shifts each
 // row by one when it stages it, so the multiplier here uses k - 1.
+// -vs_A, or with LAP |q_s|^2 vs_A (the shifted wavenumber on axis A).
 template <typename T, int A, bool LAP> struct MGrad {
   static constexpr bool kActive = true;
   StepCtx<T> c;
-  __device__ double operator()(int i, int j, int k) const {
-    if (A == 2 && k == 0) return 0.0;
-    const int ko = A == 2 ? k - 1 : k;
-    const double vs = A == 0 ? __ldg(c.vsx + i) : (A == 1 ? __ldg(c.vsy + j) : __ldg(c.vsz + ko));
-    if (!LAP) return -vs;
-    const double a = A == 0 ? vs : __ldg(c.vqx + i), b = A == 1 ? vs : __ldg(c.vqy + j),
-                 d = A == 2 ? vs : __ldg(c.vqz + ko);
-    return (a * a + b * b + d * d) * vs;   // -mq * (-vs)
+  struct Col { double vs, s; bool zero; };   // vs_A (A = 1, 2); the j, k part of |q_s|^2
+  __device__ Col col(int j, int k) const {
+    Col cl{0.0, 0.0, A == 2 && k == 0};
+    const int ko = A == 2 ? (k > 0 ? k - 1 : 0) : k;
+    const double y = A == 1 ? __ldg(c.vsy + j) : __ldg(c.vqy + j);
+    const double z = A == 2 ? __ldg(c.vsz + ko) : __ldg(c.vqz + ko);
+    if (A == 1) cl.vs = y;
+    if (A == 2) cl.vs = z;
+    cl.s = y * y + z * z;
+    return cl;
   }
+  __device__ double row(int i, const Col& cl) const {
+    if (A == 2 && cl.zero) return 0.0;
+    if (!LAP) return A == 0 ? -__ldg(c.vsx + i) : -cl.vs;
+    const double x = A == 0 ? __ldg(c.vsx + i) : __ldg(c.vqx + i);
+    return (x * x + cl.s) * (A == 0 ? x : cl.vs);   // -mq * (-vs)
+  }
+  __device__ double operator()(int i, int j, int k) const { return row(i, col(j, k)); }
 };
 
 // ---------------------------------------------------------------------------
