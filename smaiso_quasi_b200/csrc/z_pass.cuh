@@ -247,7 +247,8 @@ struct ZTile {
 
 // Stages 1 .. last of the tile after the first stage's writes, then (forward)
 // the unpack: `ex.phase(rd, wr, ...)` as in r2r_core.cuh.  Leaves the dense
-// output rows in `stg` (which overlays `cb`) with a barrier after them.
+// output rows in `stg` (which overlays `cb`) without a closing barrier: the
+// caller fences them for the TMA store and synchronises.
 template <typename T, int N, int G, int NT, int ST, class Exec>
 QHD void ztile_rest(Exec& ex, int tid, int kind, Cx<T>* cb, T* stg, Tables<T> tb) {
   using Z = ZTile<T, N, G, NT>;
@@ -259,7 +260,7 @@ QHD void ztile_rest(Exec& ex, int tid, int kind, Cx<T>* cb, T* stg, Tables<T> tb
     Regs regs;
     if (last && !is_forward(kind)) {
       ex.phase([&](int t, Regs& rg) { Z::template stage_read<R, n, s>(t, cb, tb, rg); },
-               [&](int t, Regs& rg) { Z::template last_write_inv<R, s>(t, stg, kind, rg); }, tid, regs, true, true);
+               [&](int t, Regs& rg) { Z::template last_write_inv<R, s>(t, stg, kind, rg); }, tid, regs, true, false);
       return;
     }
     ex.phase([&](int t, Regs& rg) { Z::template stage_read<R, n, s>(t, cb, tb, rg); },
@@ -267,7 +268,7 @@ QHD void ztile_rest(Exec& ex, int tid, int kind, Cx<T>* cb, T* stg, Tables<T> tb
     if constexpr (last) {
       typename Z::UnpackRegs ur;
       ex.phase([&](int t, typename Z::UnpackRegs& rg) { Z::unpack_read(t, cb, tb, rg); },
-               [&](int t, typename Z::UnpackRegs& rg) { Z::unpack_write(t, stg, kind, rg); }, tid, ur, true, true);
+               [&](int t, typename Z::UnpackRegs& rg) { Z::unpack_write(t, stg, kind, rg); }, tid, ur, true, false);
     } else {
       ztile_rest<T, N, G, NT, ST + 1>(ex, tid, kind, cb, stg, tb);
     }
@@ -286,7 +287,7 @@ QHD void ztile_after_first(Exec& ex, int tid, int kind, Cx<T>* cb, T* stg, Table
     if (is_forward(kind)) {
       typename Z::UnpackRegs ur;
       ex.phase([&](int t, typename Z::UnpackRegs& rg) { Z::unpack_read(t, cb, tb, rg); },
-               [&](int t, typename Z::UnpackRegs& rg) { Z::unpack_write(t, stg, kind, rg); }, tid, ur, true, true);
+               [&](int t, typename Z::UnpackRegs& rg) { Z::unpack_write(t, stg, kind, rg); }, tid, ur, true, false);
     } else {
       struct One {
         T x[(G * N + NT - 1) / NT], y[(G * N + NT - 1) / NT];
@@ -310,7 +311,7 @@ QHD void ztile_after_first(Exec& ex, int tid, int kind, Cx<T>* cb, T* stg, Table
               Z::put_inv(stg, kind, g, k, Cx<T>{o.x[c], o.y[c]});
             }
           },
-          tid, one, true, true);
+          tid, one, true, false);
     }
   }
 }
@@ -408,7 +409,7 @@ __global__ void __launch_bounds__(256, 2)
     Z::template stage_write<Z::R1, 1>(tid, cb, r1);
     __syncthreads();
     ztile_after_first<T, N, G, NT>(ex, tid, kind, cb, stg, tb);
-    // staging rows complete (barrier above): hand them to the async proxy
+    // this thread's staging writes to the async proxy, then every thread's
     fence_proxy_async_smem();
     __syncthreads();
     if (tid == 0) {
