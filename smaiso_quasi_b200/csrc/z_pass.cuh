@@ -26,9 +26,17 @@
 
 namespace quasi {
 
-template <typename T, int N, int G, int NT>
+// SUB: the dense rows are held as SUB blocks [SUB][2G][N/SUB] (a TMA box side
+// is at most 256 elements, so N = 512 moves as two boxes per row).
+template <typename T, int N, int G, int NT, int SUB = 1>
 struct ZTile {
   static constexpr RadixPlan plan = radix_plan(N, max_radix<T>());
+  static constexpr int BN = N / SUB;
+  static_assert(BN * SUB == N, "SUB divides N");
+  // element n of dense row r
+  QHD static constexpr int ri(int r, int n) {
+    return SUB == 1 ? r * N + n : (n / BN) * (2 * G * BN) + r * BN + (n - (n / BN) * BN);
+  }
   static_assert(plan.n_stages > 0, "unsupported transform length");
   static constexpr int R1 = plan.r[0];
   QHD static constexpr int phi(int e) { return e + e / R1; }
@@ -49,14 +57,14 @@ struct ZTile {
   struct Rows {
     const T* raw;
     int ks;
-    QHD T at(int r, int n) const { return n + ks < N ? raw[r * N + n + ks] : T(0); }
+    QHD T at(int r, int n) const { return n + ks < N ? raw[ri(r, n + ks)] : T(0); }
   };
   // the same with the shift fixed at compile time (the kernel's form)
   template <int KS> struct RowsK {
     const T* raw;
     QHD T at(int r, int n) const {
-      if constexpr (KS == 0) return raw[r * N + n];
-      else return n + KS < N ? raw[r * N + n + KS] : T(0);
+      if constexpr (KS == 0) return raw[ri(r, n)];
+      else return n + KS < N ? raw[ri(r, n + KS)] : T(0);
     }
   };
   template <class Src>
@@ -166,8 +174,8 @@ struct ZTile {
     T sgn = T(1);
     if (k < N / 2) n = 2 * k;
     else { n = 2 * (N - 1 - k) + 1; if (kind == O01) sgn = T(-1); }
-    stg[(2 * g) * N + n] = sgn * f.x;
-    stg[(2 * g + 1) * N + n] = -sgn * f.y;
+    stg[ri(2 * g, n)] = sgn * f.x;
+    stg[ri(2 * g + 1, n)] = -sgn * f.y;
   }
   template <int R, int s>
   QHD static void last_write_inv(int tid, T* stg, int kind, const Regs<R>& r) {
@@ -233,14 +241,12 @@ struct ZTile {
       const int w = tid + c * NT;
       if (w >= G * H) break;
       const int g = w / H, k = w - g * H;
-      T* ra = stg + (2 * g) * N;
-      T* rb = stg + (2 * g + 1) * N;
       auto idx = [&](int kk) { return kind == O10 ? N - 1 - kk : kk; };
-      ra[idx(k)] = r.ya[c][0];
-      rb[idx(k)] = r.yb[c][0];
+      stg[ri(2 * g, idx(k))] = r.ya[c][0];
+      stg[ri(2 * g + 1, idx(k))] = r.yb[c][0];
       const int k1 = k ? N - k : H;
-      ra[idx(k1)] = r.ya[c][1];
-      rb[idx(k1)] = r.yb[c][1];
+      stg[ri(2 * g, idx(k1))] = r.ya[c][1];
+      stg[ri(2 * g + 1, idx(k1))] = r.yb[c][1];
     }
   }
 };
@@ -249,9 +255,9 @@ struct ZTile {
 // the unpack: `ex.phase(rd, wr, ...)` as in r2r_core.cuh.  Leaves the dense
 // output rows in `stg` (which overlays `cb`) without a closing barrier: the
 // caller fences them for the TMA store and synchronises.
-template <typename T, int N, int G, int NT, int ST, class Exec>
+template <typename T, int N, int G, int NT, int ST, int SUB = 1, class Exec>
 QHD void ztile_rest(Exec& ex, int tid, int kind, Cx<T>* cb, T* stg, Tables<T> tb) {
-  using Z = ZTile<T, N, G, NT>;
+  using Z = ZTile<T, N, G, NT, SUB>;
   if constexpr (ST < Z::plan.n_stages) {
     constexpr int R = Z::plan.r[ST];
     constexpr int s = stage_stride(N, ST, max_radix<T>()), n = N / s;
@@ -270,18 +276,18 @@ QHD void ztile_rest(Exec& ex, int tid, int kind, Cx<T>* cb, T* stg, Tables<T> tb
       ex.phase([&](int t, typename Z::UnpackRegs& rg) { Z::unpack_read(t, cb, tb, rg); },
                [&](int t, typename Z::UnpackRegs& rg) { Z::unpack_write(t, stg, kind, rg); }, tid, ur, true, false);
     } else {
-      ztile_rest<T, N, G, NT, ST + 1>(ex, tid, kind, cb, stg, tb);
+      ztile_rest<T, N, G, NT, ST + 1, SUB>(ex, tid, kind, cb, stg, tb);
     }
   }
 }
 
 // Single-stage plans (N = R1) end in the first stage: its output goes through
 // the padded tile so that the write above stays uniform.
-template <typename T, int N, int G, int NT, class Exec>
+template <typename T, int N, int G, int NT, int SUB = 1, class Exec>
 QHD void ztile_after_first(Exec& ex, int tid, int kind, Cx<T>* cb, T* stg, Tables<T> tb) {
-  using Z = ZTile<T, N, G, NT>;
+  using Z = ZTile<T, N, G, NT, SUB>;
   if constexpr (Z::plan.n_stages > 1) {
-    ztile_rest<T, N, G, NT, 1>(ex, tid, kind, cb, stg, tb);
+    ztile_rest<T, N, G, NT, 1, SUB>(ex, tid, kind, cb, stg, tb);
   } else {
     // the first stage wrote Z (or F) in natural order: finish like a last stage
     if (is_forward(kind)) {
@@ -316,6 +322,10 @@ QHD void ztile_after_first(Exec& ex, int tid, int kind, Cx<T>* cb, T* stg, Table
   }
 }
 
+// Shared-memory copy of the full root table for the later stages: FP32 only
+// (it measured neutral for FP64, whose N = 512 tile would not fit twice per SM).
+template <typename T> constexpr bool zpass_root_copy() { return sizeof(T) == 4; }
+
 #ifdef __CUDACC__
 __device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, const void* src, int c0, int c1, int c2) {
   asm volatile(
@@ -330,7 +340,8 @@ __device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.
 // all committed bulk stores are complete
 __device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 
-// Persistent z pass: tiles of P = 2G consecutive rows (P divides ny), N <= 256.
+// Persistent z pass: tiles of P = 2G consecutive rows (P divides ny), N <= 512
+// (N = 512 moves each row as two 256-element boxes, held [2][P][256]).
 // Shared memory: two dense landing buffers (TMA loads) and the padded complex
 // tile, whose first P * N elements double as the dense staging rows of the
 // TMA store.  One thread issues all copies; the landing buffer of tile t is
@@ -340,8 +351,9 @@ template <typename T, int N, int P, int KS>
 __global__ void __launch_bounds__(256, 2)
     tma_zpass_kernel(const __grid_constant__ CUtensorMap src_map, const __grid_constant__ CUtensorMap dst_map, Geom g,
                      int kind, Tables<T> tb, int ntiles, int* err) {
-  constexpr int NT = 256, G = P / 2;
-  using Z = ZTile<T, N, G, NT>;
+  constexpr int NT = 256, G = P / 2, SUB = (N + 255) / 256, BN = N / SUB;
+  using Z = ZTile<T, N, G, NT, SUB>;
+  constexpr bool kRootCopy = zpass_root_copy<T>();
   extern __shared__ __align__(128) unsigned char smem_raw[];
   T* raw0 = reinterpret_cast<T*>(smem_raw);
   T* raw1 = raw0 + P * N;
@@ -352,7 +364,7 @@ __global__ void __launch_bounds__(256, 2)
   // table the pre-twiddle and the unpack read
   Cx<T>* tw1 = reinterpret_cast<Cx<T>*>(bar + 2);
   Cx<T>* qt = tw1 + N;
-  Cx<T>* rt = qt + N;   // the root table itself, for the later stages
+  Cx<T>* rt = qt + N;   // FP32: the root table itself, for the later stages
   const int tid = threadIdx.x;
   {
     constexpr int M = N / Z::R1;
@@ -360,10 +372,10 @@ __global__ void __launch_bounds__(256, 2)
       const int u = e / M, b = e - u * M;
       tw1[e] = tb.root[b * u];
       qt[e] = tb.quarter[e];
-      rt[e] = tb.root[e];
+      if constexpr (kRootCopy) rt[e] = tb.root[e];
     }
     tb.quarter = qt;
-    tb.root = rt;
+    if constexpr (kRootCopy) tb.root = rt;
   }
   auto origin = [&](int t, int& c1, int& c2) {
     const int row = t * P;
@@ -374,7 +386,8 @@ __global__ void __launch_bounds__(256, 2)
     int c1, c2;
     origin(t, c1, c2);
     mbar_expect_tx(b, uint32_t(P) * N * sizeof(T));
-    tma_load_3d(dst, &src_map, b, 0, c1, c2);
+#pragma unroll
+    for (int sb = 0; sb < SUB; ++sb) tma_load_3d(dst + sb * P * BN, &src_map, b, sb * BN, c1, c2);
   };
   if (tid == 0) {
     mbar_init(&bar[0], 1);
@@ -408,14 +421,15 @@ __global__ void __launch_bounds__(256, 2)
     }
     Z::template stage_write<Z::R1, 1>(tid, cb, r1);
     __syncthreads();
-    ztile_after_first<T, N, G, NT>(ex, tid, kind, cb, stg, tb);
+    ztile_after_first<T, N, G, NT, SUB>(ex, tid, kind, cb, stg, tb);
     // this thread's staging writes to the async proxy, then every thread's
     fence_proxy_async_smem();
     __syncthreads();
     if (tid == 0) {
       int c1, c2;
       origin(t, c1, c2);
-      tma_store_3d(&dst_map, stg, 0, c1, c2);
+#pragma unroll
+      for (int sb = 0; sb < SUB; ++sb) tma_store_3d(&dst_map, stg + sb * P * BN, sb * BN, c1, c2);
       bulk_commit();
     }
   }
@@ -428,15 +442,16 @@ __global__ void __launch_bounds__(256, 2)
 
 template <typename T, int N, int KS>
 cudaError_t launch_zpass_nk(const Geom& g, int kind, Tables<T> tb, const T* src, T* dst, cudaStream_t s) {
-  constexpr int P = pass_pencils<T>(N), G = P / 2;
-  using Z = ZTile<T, N, G, 256>;
+  constexpr int P = pass_pencils<T>(N), G = P / 2, SUB = (N + 255) / 256;
+  using Z = ZTile<T, N, G, 256, SUB>;
   if (g.ny % P != 0) return cudaErrorNotSupported;
-  const uint32_t box[3] = {uint32_t(N), uint32_t(P), 1};
+  const uint32_t box[3] = {uint32_t(N / SUB), uint32_t(P), 1};
   CUtensorMap smap, dmap;
   if (!MapCache::get().lookup(&smap, src, int(sizeof(T)), g.nx, g.ny, g.nz, 2, box) ||
       !MapCache::get().lookup(&dmap, dst, int(sizeof(T)), g.nx, g.ny, g.nz, 2, box))
     return cudaErrorNotSupported;
-  const size_t smem = size_t(2) * P * N * sizeof(T) + ((Z::cb_bytes() + 15) / 16) * 16 + 16 + 3 * N * sizeof(Cx<T>);
+  const size_t smem = size_t(2) * P * N * sizeof(T) + ((Z::cb_bytes() + 15) / 16) * 16 + 16 +
+                      (zpass_root_copy<T>() ? 3 : 2) * N * sizeof(Cx<T>);
   auto kern = tma_zpass_kernel<T, N, P, KS>;
   static int per_sm = 0;   // per instantiation
   if (per_sm == 0) {
@@ -472,6 +487,7 @@ cudaError_t launch_zpass(const Geom& g, int kind, Tables<T> tb, const T* src, T*
     case 128: return launch_zpass_n<T, 128>(g, kind, tb, src, dst, s, ks);
     case 192: return launch_zpass_n<T, 192>(g, kind, tb, src, dst, s, ks);
     case 256: return launch_zpass_n<T, 256>(g, kind, tb, src, dst, s, ks);
+    case 512: return launch_zpass_n<T, 512>(g, kind, tb, src, dst, s, ks);
     default: return cudaErrorNotSupported;
   }
 }

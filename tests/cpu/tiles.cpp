@@ -89,8 +89,8 @@ template <typename T, int N, int G, int NT> double tile_case(int kind, bool inpl
   return worst(kind, N, P, X, LD, Y.data(), LD, 0);
 }
 
-template <typename T, int N, int G, int NT> double ztile_case(int kind, int ks) {
-  using Z = ZTile<T, N, G, NT>;
+template <typename T, int N, int G, int NT, int SUB = 1> double ztile_case(int kind, int ks) {
+  using Z = ZTile<T, N, G, NT, SUB>;
   std::mt19937_64 rng(N * 11 + kind);
   std::uniform_real_distribution<double> U(-1, 1);
   Tabs<T> tb(N);
@@ -103,8 +103,15 @@ template <typename T, int N, int G, int NT> double ztile_case(int kind, int ks) 
   for (int t = 0; t < NT; ++t) Z::first_read(t, typename Z::Rows{raw.data(), ks}, kind, tb.get(), r1[t]);
   for (int t = 0; t < NT; ++t) Z::template stage_write<Z::R1, 1>(t, cb.data(), r1[t]);
   HostExec<NT> ex;
-  ztile_after_first<T, N, G, NT>(ex, 0, kind, cb.data(), stg, tb.get());
-  return worst(kind, N, P, raw, N, stg, N, ks);
+  ztile_after_first<T, N, G, NT, SUB>(ex, 0, kind, cb.data(), stg, tb.get());
+  // rows as [p][n] whatever the block layout
+  std::vector<T> xd(P * N), od(P * N);
+  for (int p = 0; p < P; ++p)
+    for (int n = 0; n < N; ++n) {
+      xd[p * N + n] = raw[Z::ri(p, n)];
+      od[p * N + n] = stg[Z::ri(p, n)];
+    }
+  return worst(kind, N, P, xd, N, od.data(), N, ks);
 }
 
 template <typename T, int N, int G, int NT> void tiles() {
@@ -112,10 +119,11 @@ template <typename T, int N, int G, int NT> void tiles() {
   for (int k = 0; k < 4; k++) w = std::max({w, tile_case<T, N, G, NT>(k, true), tile_case<T, N, G, NT>(k, false)});
   printf("tile %s %d %.3g\n", sizeof(T) == 8 ? "f64" : "f32", N, w);
 }
-template <typename T, int N, int G> void ztiles() {
+template <typename T, int N, int G, int SUB = 1> void ztiles() {
   double w = 0;
-  for (int k = 0; k < 4; k++) w = std::max({w, ztile_case<T, N, G, 256>(k, 0), ztile_case<T, N, G, 256>(k, 1)});
-  printf("ztile %s %d %.3g\n", sizeof(T) == 8 ? "f64" : "f32", N, w);
+  for (int k = 0; k < 4; k++)
+    w = std::max({w, ztile_case<T, N, G, 256, SUB>(k, 0), ztile_case<T, N, G, 256, SUB>(k, 1)});
+  printf("ztile %s %d %.3g\n", sizeof(T) == 8 ? "f64" : "f32", N * 10 + SUB, w);
 }
 
 int main() {
@@ -126,5 +134,6 @@ int main() {
   ztiles<double, 128, 8>(); ztiles<double, 192, 8>(); ztiles<double, 256, 8>(); ztiles<double, 8, 8>();
   ztiles<float, 16, 16>(); ztiles<float, 64, 16>(); ztiles<float, 96, 16>(); ztiles<float, 128, 16>();
   ztiles<float, 192, 16>(); ztiles<float, 256, 16>();
+  ztiles<double, 512, 4, 2>(); ztiles<float, 512, 8, 2>();   // two 256-element blocks per row
   return 0;
 }

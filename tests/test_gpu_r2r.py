@@ -7,7 +7,8 @@ from oracle import quasi_oracle as qo
 
 pytestmark = pytest.mark.gpu
 
-GRIDS = [(16, 16, 32), (8, 16, 16), (32, 64, 16), (96, 96, 192), (64, 64, 128), (128, 32, 256), (512, 16, 32)]
+GRIDS = [(16, 16, 32), (8, 16, 16), (32, 64, 16), (96, 96, 192), (64, 64, 128), (128, 32, 256), (512, 16, 32),
+         (16, 32, 512)]
 
 
 def rel(a, b):
@@ -26,7 +27,7 @@ def test_r2r_fp64_matches_fftw_kinds(grid, plan):
     assert rel(got, ref) < 1e-14
 
 
-@pytest.mark.parametrize("grid", [(16, 16, 32), (64, 64, 128), (96, 96, 192)])
+@pytest.mark.parametrize("grid", [(16, 16, 32), (64, 64, 128), (96, 96, 192), (16, 32, 512)])
 @pytest.mark.parametrize("plan", ["CT", "iCT", "STx", "iSTz"])
 def test_r2r_fp32_error(grid, plan):
     import smaiso_quasi_b200 as q

@@ -86,7 +86,7 @@ def test_step_fp64_crosses_divv_and_pressure_switches():
         compare(sim, o, 1e-11)
 
 
-@pytest.mark.parametrize("grid", [(32, 32, 64), (24 * 4, 24 * 4, 24 * 8)])
+@pytest.mark.parametrize("grid", [(32, 32, 64), (24 * 4, 24 * 4, 24 * 8), (16, 16, 512)])
 def test_step_fp64_larger_grids(grid):
     if grid[0] == 96:
         grid = (96, 96, 192)

@@ -26,12 +26,12 @@ def results(tmp_path_factory):
 
 def test_every_case_ran(results):
     assert sum(1 for k in results if k[0] == "tile") == 12
-    assert sum(1 for k in results if k[0] == "ztile") == 14
+    assert sum(1 for k in results if k[0] == "ztile") == 16
 
 
 @pytest.mark.parametrize("family", ["tile", "ztile"])
 def test_tiles_match_the_definitions(results, family):
-    for (fam, typ, n), err in results.items():
+    for (fam, typ, n), err in results.items():   # ztile n: 10 N + row blocks
         if fam != family:
             continue
         tol = 1e-14 if typ == "f64" else 1e-6
