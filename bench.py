@@ -1,9 +1,12 @@
 """Throughput of the quasi-incompressible smectic-isotropic step at 256^3.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                    [--workload interface256|droplet512]
 
 Workload: the planar smectic-isotropic interface at 256x256x256 (seeded
-+-1e-3 noise), the reference's quasi.cpp model at its default coefficients.
++-1e-3 noise), the reference's quasi.cpp model at its default coefficients,
+FP32 against FP64 after its 1000 steps; --workload droplet512: a smectic
+droplet (r = 0.3 L) at 512x512x512, compared after its 200 steps.
 One "step" is one time step of the whole model (24 r2r transforms plus the
 fused pointwise stages).  The chosen form (FP32 fields and transforms, FP64
 constants/update/reductions) is the headline; the plain FP64 form is timed on
@@ -43,6 +46,16 @@ sys.path.insert(0, str(ROOT))
 GRID = (256, 256, 256)
 METRIC = "steps/s @256^3: plain FP64 vs FP32/split-BF16 TC; % HBM roofline; err vs FP64"
 WORKLOAD = "planar smectic-isotropic interface 256x256x256, quasi.cpp model, seeded +-1e-3 noise"
+IC_KIND = "planar"
+
+# --workload: the headline case above, or the 512^3 droplet run (r = 0.3 L,
+# 200 steps) the same line is measured on with --workload droplet512
+WORKLOADS = {
+    "interface256": ((256, 256, 256), "planar", METRIC, WORKLOAD, 1000),
+    "droplet512": ((512, 512, 512), "droplet",
+                   "steps/s @512^3 droplet: plain FP64 vs FP32; % HBM roofline; err vs FP64",
+                   "smectic droplet r = 0.3 L in the isotropic melt 512x512x512, quasi.cpp model, seeded", 200),
+}
 
 
 def peaks() -> dict:
@@ -66,10 +79,17 @@ class ClockSampler:
         self.tmp = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
 
     def __enter__(self):
+        self.mark = 0
         if shutil.which("nvidia-smi"):
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
                                          stdout=self.tmp, stderr=subprocess.DEVNULL)
+            # the timed region starts once the sampler is running (first sample
+            # written); only the samples after this point are summarised
+            t_end = time.time() + 10
+            while time.time() < t_end and os.path.getsize(self.tmp.name) == 0 and self.proc.poll() is None:
+                time.sleep(0.02)
+            self.mark = os.path.getsize(self.tmp.name)
         return self
 
     def __exit__(self, *exc):
@@ -83,7 +103,10 @@ class ClockSampler:
     def summary(self) -> dict:
         self.tmp.flush()
         rows = []
-        for line in open(self.tmp.name):
+        with open(self.tmp.name) as f:
+            f.seek(self.mark)
+            lines = f.read().splitlines()
+        for line in lines:
             parts = [x.strip() for x in line.split(",")]
             if len(parts) >= 9:
                 rows.append(parts)
@@ -137,10 +160,10 @@ def run_profile_case(args) -> None:
     the committed ncu summaries capture."""
     import smaiso_quasi_b200 as q
     cfg, sim = make_sim(q, args.precision, 0)
-    sim.set_psi(q.initial_condition(cfg, "planar", seed=1234))
+    sim.set_psi(q.initial_condition(cfg, IC_KIND, seed=1234))
     sim.init()
     sim.step(args.warmup + args.steps)
-    print(json.dumps({"profile_case": f"{args.precision} 256^3", "steps": args.warmup + args.steps,
+    print(json.dumps({"profile_case": f"{args.precision} {GRID[0]}^3", "steps": args.warmup + args.steps,
                       "axis": args.axis, "pass_ms": sim.time_axis_pass(args.axis, reps=3)}))
 
 
@@ -156,7 +179,7 @@ def run_gpu(args) -> None:
     pk = peaks()
 
     cfg32, s32 = make_sim(q, "fp32", device)
-    psi0 = q.initial_condition(cfg32, "planar", seed=1234)
+    psi0 = q.initial_condition(cfg32, IC_KIND, seed=1234)
 
     # ---- e2e through the public C ABI, host buffers, copies inside ----------
     # set_psi (H2D of the initial field) + init + K steps with the reference's
@@ -204,10 +227,12 @@ def run_gpu(args) -> None:
     traffic = None
     prof = ROOT / "profiles" / "traffic.json"
     if prof.exists():
-        traffic = json.loads(prof.read_text()).get("y_pass_fp32_256_bytes_per_launch")
+        # captured at 256^3; other grids scale it by the cells a launch processes
+        t256 = json.loads(prof.read_text()).get("y_pass_fp32_256_bytes_per_launch")
+        traffic = None if t256 is None else int(t256 * n_cells / 256 ** 3)
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": pk["hbm_gbs"], "unit": "GB/s",
                 "frac": round(achieved / pk["hbm_gbs"], 4), "traffic": traffic,
-                "kernel": "tma_pass_kernel<float,256,1,32> (plain y pass)",
+                "kernel": f"tma_pass_kernel<float,{GRID[1]},1,P> (plain y pass)",
                 "peak_source": pk["source"] + " (burst copy)"}
     b_alg32 = 48 * 4 * n_cells
     step_roofline = {"b_alg_bytes": b_alg32, "achieved_gbs": round(b_alg32 * steps_per_s / args.gpus / 1e9, 1),
@@ -224,7 +249,7 @@ def run_gpu(args) -> None:
     b_alg64 = 48 * 8 * n_cells
 
     # error of the FP32 form against FP64 from the same IC, after the
-    # workload's 1000 steps (both continue untimed past the timed window)
+    # workload's run length (both continue untimed past the timed window)
     n_err = max(W + K, args.err_steps)
     if n_err > W + K:
         s32.step(n_err - (W + K))
@@ -270,7 +295,7 @@ def run_gpu(args) -> None:
 
 def cpu_baseline(samples: int) -> dict | None:
     """The reference's own quasi.cpp on the host cores: `samples` steps of the
-    256^3 grid (its focal-conic IC; the per-step work does not depend on psi),
+    workload's grid (its focal-conic IC; the per-step work does not depend on psi),
     loop wall time as the reference itself reports it (quasi.cpp:2298-2304)."""
     from oracle import ref_runner as rr
     if not rr.available("quasi"):
@@ -285,7 +310,7 @@ def cpu_baseline(samples: int) -> dict | None:
     m = re.findall(r"Finished in ([0-9.eE+-]+) seconds \[Wall Clock\]", r["stdout"])
     loop_s = float(m[-1]) if m else r["wall_s"]
     return {"value": round(samples / loop_s, 5), "unit": "steps/s", "cores": ranks, "kind": "reference",
-            "sample": f"{samples} step(s) of 256^3, reference quasi.cpp built on oracle/shim "
+            "sample": f"{samples} step(s) of {GRID[0]}x{GRID[1]}x{GRID[2]}, reference quasi.cpp built on oracle/shim "
                       f"(FFTW r2r restated, {ranks} MPI ranks as threads), loop wall time"}
 
 
@@ -312,15 +337,24 @@ def run_reference(args) -> None:
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default: 400 at 256^3, 100 at 512^3: about a second of FP32 steps or more)")
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--err-steps", type=int, default=1000, help="steps after which FP32 is compared with FP64")
+    ap.add_argument("--err-steps", type=int, default=None,
+                    help="steps after which FP32 is compared with FP64 (default: the workload's run length)")
+    ap.add_argument("--workload", default="interface256", choices=sorted(WORKLOADS))
     ap.add_argument("--profile", action="store_true", help="one engine only (for ncu captures)")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"], help="engine of --profile")
     ap.add_argument("--axis", type=int, default=1, choices=[0, 1, 2], help="pass timed at the end of --profile")
     args = ap.parse_args()
+    global GRID, IC_KIND, METRIC, WORKLOAD
+    GRID, IC_KIND, METRIC, WORKLOAD, run_len = WORKLOADS[args.workload]
+    if args.err_steps is None:
+        args.err_steps = run_len
+    if args.steps is None:
+        args.steps = 400 if GRID[0] <= 256 else 100
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
