@@ -384,6 +384,9 @@ template <class S, class = void> struct SrcAliasesTile {
 template <class S> struct SrcAliasesTile<S, std::void_t<decltype(S::kAliasesTile)>> {
   static constexpr bool value = S::kAliasesTile;
 };
+// The same for a sink: the last stage (or the unpack) then reads everything
+// before it writes.
+template <class S> using SnkAliasesTile = SrcAliasesTile<S>;
 
 // `hook()` runs on every thread right after the first stage's closing barrier
 // (the moment the first stage's input is no longer needed).
@@ -403,7 +406,7 @@ QHD void r2r_stages(Exec& ex, int tid, int kind, Cx<T>* cb, const Src& src, cons
     // shared buffer; otherwise only for middle stages and a forward kind's
     // last stage (both write the shared buffer they read)
     const bool global_out = last && !is_forward(kind);
-    const bool mid = INPLACE || (first ? SrcAliasesTile<Src>::value : !global_out);
+    const bool mid = INPLACE || (first ? SrcAliasesTile<Src>::value : (!global_out || SnkAliasesTile<Snk>::value));
     // a write half must be visible before the next read half; an inverse
     // kind's last stage writing to global memory is followed by nothing
     const bool after = !last || is_forward(kind) || INPLACE;
@@ -427,8 +430,8 @@ QHD void r2r_tile(Exec& ex, int tid, int kind, Cx<T>* cb, const Src& src, const 
   if (is_forward(kind)) {
     typename F::UnpackRegs regs;
     ex.phase([&](int t, typename F::UnpackRegs& rg) { F::unpack_read(t, cb, tb, rg); },
-             [&](int t, typename F::UnpackRegs& rg) { F::unpack_write(t, snk, kind, rg); }, tid, regs, INPLACE,
-             INPLACE);
+             [&](int t, typename F::UnpackRegs& rg) { F::unpack_write(t, snk, kind, rg); }, tid, regs,
+             INPLACE || SnkAliasesTile<Snk>::value, INPLACE);
   }
 }
 

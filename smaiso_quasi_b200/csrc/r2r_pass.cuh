@@ -254,6 +254,21 @@ struct RawSrc {
   }
 };
 
+// x / y tile sink for a TMA store: pencils 2g, 2g+1 at position n into the
+// staging rows [n][P] (the store box's layout), which overlay the work tile.
+template <typename T>
+struct RowStageSnk {
+  static constexpr bool kAliasesTile = true;
+  T* stg;
+  int P;
+  QHD void put(int g, int n, T a, T b) const {
+    typename Vec2<T>::type v;
+    v.x = a;
+    v.y = b;
+    *reinterpret_cast<typename Vec2<T>::type*>(stg + n * P + 2 * g) = v;
+  }
+};
+
 // Identity multiplier (plain passes).
 struct NoMul {
   static constexpr bool kActive = false;
@@ -357,10 +372,17 @@ template <bool IP> constexpr int tma_min_blocks() { return IP ? 3 : 2; }
 // Mul2 != NoMul (x / y, not IP): each tile, loaded once, is transformed twice,
 // with mul into st and with mul2 into st2 (two inverse transforms of the same
 // spectral field that differ only in their multiplier).
-template <typename T, int N, int AXIS, int P, class Store, class Mul, bool IP = false, class Mul2 = NoMul>
+// TSTORE (plain field outputs, not IP): the last stage writes the staging rows
+// over the work tile and one thread stores the tile through dmap (dmap2 for
+// the dual pass's second output); the next tile's first stage waits for the
+// store to have read them.
+template <typename T, int N, int AXIS, int P, class Store, class Mul, bool IP = false, class Mul2 = NoMul,
+          bool TSTORE = false>
 __global__ void __launch_bounds__(tma_threads<T>(), tma_min_blocks<IP>())
     tma_pass_kernel(const __grid_constant__ CUtensorMap map, Geom g, int kind, Tables<T> tb, Store st, int ntiles,
-                    int* err, Mul mul, int dc1, int dc2, int ks, Store st2, Mul2 mul2) {
+                    int* err, Mul mul, int dc1, int dc2, int ks, Store st2, Mul2 mul2,
+                    const __grid_constant__ CUtensorMap dmap, const __grid_constant__ CUtensorMap dmap2) {
+  static_assert(!TSTORE || (!IP && AXIS != 2), "TMA-stored tiles are x / y passes with a work tile");
   static_assert(!IP || AXIS != 2, "in-place raw tiles are for x / y passes");
   constexpr bool kDual = !std::is_same<Mul2, NoMul>::value;
   static_assert(tma_threads<T>() % (P / 2) == 0, "MulSrc::prep: each thread reads one pencil pair");
@@ -404,11 +426,31 @@ __global__ void __launch_bounds__(tma_threads<T>(), tma_min_blocks<IP>())
     const uint32_t parity = (it >> 1) & 1;
     // every thread polls; the CTA leaves together if any poll gave up
     const bool arrived = mbar_wait_bounded(&bar[b], parity, kTmaPollLimit);
+    if constexpr (TSTORE) {
+      if (tid == 0) bulk_wait_read0();   // the previous tile's store has read the work tile
+    }
     if (!__syncthreads_and(arrived)) {
       if (tid == 0) atomicExch(err, 1);
       break;
     }
     const int t_next = t + 2 * int(gridDim.x);
+    // TSTORE: hand the staging rows over the work tile to the async proxy and
+    // store them as the tile's box(es)
+    auto store_tile = [&](const CUtensorMap* dm) {
+      fence_proxy_async_smem();
+      __syncthreads();
+      if (tid == 0) {
+        constexpr int SUB = (N + 255) / 256, BN = N / SUB;
+        int c0, c1, c2;
+        tile_origin<AXIS, P>(g, t, c0, c1, c2);
+#pragma unroll
+        for (int sb = 0; sb < SUB; ++sb) {
+          if (AXIS == 1) tma_store_3d(dm, work + sb * BN * P, c0, c1 + sb * BN, c2);
+          else tma_store_3d(dm, work + sb * BN * P, c0, c1, c2 + sb * BN);
+        }
+        bulk_commit();
+      }
+    };
     auto issue_next = [&]() {
       if (tid == 0 && t_next < ntiles) {
         fence_proxy_async_smem();
@@ -431,20 +473,39 @@ __global__ void __launch_bounds__(tma_threads<T>(), tma_min_blocks<IP>())
       const int outer = t / kt, k0 = (t - outer * kt) * P;
       MulSrc<T, AXIS, Mul> src{raw, P, outer, k0, mul};
       src.prep(tid % (P / 2));
-      r2r_tile<T, N, P / 2, NT, false>(ex, tid, kind, reinterpret_cast<Cx<T>*>(work), src,
-                                        GlobSnk<T, AXIS, Store>{st, outer, k0}, tb);
+      if constexpr (TSTORE) {
+        r2r_tile<T, N, P / 2, NT, false>(ex, tid, kind, reinterpret_cast<Cx<T>*>(work), src,
+                                          RowStageSnk<T>{work, P}, tb);
+        store_tile(&dmap);
+        if (tid == 0) bulk_wait_read0();
+      } else {
+        r2r_tile<T, N, P / 2, NT, false>(ex, tid, kind, reinterpret_cast<Cx<T>*>(work), src,
+                                          GlobSnk<T, AXIS, Store>{st, outer, k0}, tb);
+      }
       __syncthreads();   // the second transform rewrites the work tile
       MulSrc<T, AXIS, Mul2> src2{raw, P, outer, k0, mul2};
       src2.prep(tid % (P / 2));
-      r2r_tile<T, N, P / 2, NT, false>(ex, tid, kind, reinterpret_cast<Cx<T>*>(work), src2,
-                                        GlobSnk<T, AXIS, Store>{st2, outer, k0}, tb, issue_next);
+      if constexpr (TSTORE) {
+        r2r_tile<T, N, P / 2, NT, false>(ex, tid, kind, reinterpret_cast<Cx<T>*>(work), src2,
+                                          RowStageSnk<T>{work, P}, tb, issue_next);
+        store_tile(&dmap2);
+      } else {
+        r2r_tile<T, N, P / 2, NT, false>(ex, tid, kind, reinterpret_cast<Cx<T>*>(work), src2,
+                                          GlobSnk<T, AXIS, Store>{st2, outer, k0}, tb, issue_next);
+      }
     } else if constexpr (AXIS != 2) {
       const int kt = g.nz / P;
       const int outer = t / kt, k0 = (t - outer * kt) * P;
       MulSrc<T, AXIS, Mul> src{raw, P, outer, k0, mul};
       src.prep(tid % (P / 2));
-      r2r_tile<T, N, P / 2, NT, false>(ex, tid, kind, reinterpret_cast<Cx<T>*>(work), src,
-                                        GlobSnk<T, AXIS, Store>{st, outer, k0}, tb, issue_next);
+      if constexpr (TSTORE) {
+        r2r_tile<T, N, P / 2, NT, false>(ex, tid, kind, reinterpret_cast<Cx<T>*>(work), src,
+                                          RowStageSnk<T>{work, P}, tb, issue_next);
+        store_tile(&dmap);
+      } else {
+        r2r_tile<T, N, P / 2, NT, false>(ex, tid, kind, reinterpret_cast<Cx<T>*>(work), src,
+                                          GlobSnk<T, AXIS, Store>{st, outer, k0}, tb, issue_next);
+      }
     } else {
       // dense rows -> padded in-place tile (both sides contiguous in n); ks = 1
       // stages row[n + 1] at n and zero at the top
@@ -485,6 +546,9 @@ __global__ void __launch_bounds__(tma_threads<T>(), tma_min_blocks<IP>())
       }
     }
     __syncthreads();   // the next tile's first stage overwrites `work`
+  }
+  if constexpr (TSTORE) {
+    if (tid == 0) bulk_wait0();
   }
 }
 
@@ -547,8 +611,19 @@ cudaError_t launch_tma_pass(const Geom& g, int kind, Tables<T> tb, const T* src,
   else { box[0] = P; box[1] = 1; box[2] = N / SUB; }
   CUtensorMap map;
   if (!MapCache::get().lookup(&map, src, int(sizeof(T)), g.nx, g.ny, g.nz, AXIS, box)) return cudaErrorNotSupported;
+  // plain field outputs of x / y passes leave through TMA stores (same box)
+  constexpr bool TSTORE = IsStoreField<Store>::value && AXIS != 2 && !IP;
+  CUtensorMap dmap = map, dmap2 = map;
+  if constexpr (TSTORE) {
+    if (!MapCache::get().lookup(&dmap, st.dst, int(sizeof(T)), g.nx, g.ny, g.nz, AXIS, box))
+      return cudaErrorNotSupported;
+    if constexpr (!std::is_same<Mul2, NoMul>::value) {
+      if (!MapCache::get().lookup(&dmap2, st2.dst, int(sizeof(T)), g.nx, g.ny, g.nz, AXIS, box))
+        return cudaErrorNotSupported;
+    }
+  }
   const size_t smem = tma_smem_bytes<T, N, AXIS, P, IP>();
-  auto kern = tma_pass_kernel<T, N, AXIS, P, Store, Mul, IP, Mul2>;
+  auto kern = tma_pass_kernel<T, N, AXIS, P, Store, Mul, IP, Mul2, TSTORE>;
   static int per_sm = 0;   // per instantiation: resident CTAs per SM
   if (per_sm == 0) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -564,7 +639,7 @@ cudaError_t launch_tma_pass(const Geom& g, int kind, Tables<T> tb, const T* src,
   else tiles = g.ny * (g.nz / P);
   const int grid = tiles < per_sm * tma_config().sms ? tiles : per_sm * tma_config().sms;
   kern<<<grid, tma_threads<T>(), smem, s>>>(map, g, kind, tb, st, tiles, tma_config().err, mul, dc1, dc2, ks, st2,
-                                             mul2);
+                                             mul2, dmap, dmap2);
   return cudaGetLastError();
 }
 

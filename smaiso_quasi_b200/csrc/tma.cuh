@@ -1,7 +1,7 @@
 // Tensor-memory-accelerator (TMA) tile loads for the axis passes: tensor maps
 // built on the host through the driver entry point, and the device-side
 // mbarrier / cp.async.bulk.tensor primitives (inline PTX, sm_90+ / sm_100a).
-// Loads only, one CTA each: no cluster multicast anywhere.
+// Loads and stores, one CTA each: no cluster multicast anywhere.
 #pragma once
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -63,6 +63,21 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, u
       "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
       : "memory");
 }
+
+// Tile stores: shared memory -> global through a tensor map (bulk groups,
+// committed and awaited by the issuing thread).
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, const void* src, int c0, int c1, int c2) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(
+          reinterpret_cast<uint64_t>(map)),
+      "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(src))
+      : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// the smem sources of all committed bulk stores have been read
+__device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+// all committed bulk stores are complete
+__device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 
 // ---------------------------------------------------------------------------
 // Host side: one tensor map per (field, axis) over the field as a 3-D tensor

@@ -327,19 +327,6 @@ QHD void ztile_after_first(Exec& ex, int tid, int kind, Cx<T>* cb, T* stg, Table
 template <typename T> constexpr bool zpass_root_copy() { return sizeof(T) == 4; }
 
 #ifdef __CUDACC__
-__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, const void* src, int c0, int c1, int c2) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(
-          reinterpret_cast<uint64_t>(map)),
-      "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(src))
-      : "memory");
-}
-__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-// the smem sources of all committed bulk stores have been read
-__device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
-// all committed bulk stores are complete
-__device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
-
 // Persistent z pass: tiles of P = 2G consecutive rows (P divides ny), N <= 512
 // (N = 512 moves each row as two 256-element boxes, held [2][P][256]).
 // Shared memory: two dense landing buffers (TMA loads) and the padded complex
