@@ -79,6 +79,9 @@ class Engine : public EngineBase {
     for (auto& t : tw_) t.release();
     if (ev0_) cudaEventDestroy(ev0_);
     if (ev1_) cudaEventDestroy(ev1_);
+    for (auto& e : fork_ev_)
+      if (e) cudaEventDestroy(e);
+    if (stream2_) cudaStreamDestroy(stream2_);
     if (stream_) cudaStreamDestroy(stream_);
   }
 
@@ -88,6 +91,10 @@ class Engine : public EngineBase {
     g_ = Geom{cfg_.nx, cfg_.ny, cfg_.nz};
     n_ = size_t(g_.nx) * g_.ny * g_.nz;
     if (!cuda_ok(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "stream")) return QUASI_ERR_CUDA;
+    // second capture stream and fork/join events of the step graphs
+    if (!cuda_ok(cudaStreamCreateWithFlags(&stream2_, cudaStreamNonBlocking), "stream")) return QUASI_ERR_CUDA;
+    for (auto& e : fork_ev_)
+      if (!cuda_ok(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event")) return QUASI_ERR_CUDA;
     if (!cuda_ok(cudaEventCreate(&ev0_), "event") || !cuda_ok(cudaEventCreate(&ev1_), "event")) return QUASI_ERR_CUDA;
     const size_t bytes = size_t(kFields) * n_ * sizeof(T);
     if (cudaMalloc(&slab_, bytes) != cudaSuccess) {
@@ -437,7 +444,7 @@ class Engine : public EngineBase {
     use_tma();
     if (!cuda_ok(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture"))
       return QUASI_ERR_CUDA;
-    cudaError_t e = enqueue_step<T>(c_, tb_, nloop_dev_, stream_);
+    cudaError_t e = enqueue_step<T>(c_, tb_, nloop_dev_, stream_, stream2_, fork_ev_);
     cudaError_t e2 = cudaStreamEndCapture(stream_, &graph);
     if (!cuda_ok(e, "enqueue step") || !cuda_ok(e2, "end capture")) {
       if (graph) cudaGraphDestroy(graph);
@@ -468,6 +475,8 @@ class Engine : public EngineBase {
   double* tabs_ = nullptr;
   int* nloop_dev_ = nullptr;
   double* partial_ = nullptr;
+  cudaStream_t stream2_ = nullptr;
+  cudaEvent_t fork_ev_[6] = {};
   int* tma_err_ = nullptr;
   int sms_ = 148;
   bool fused_yz_ = false;

@@ -640,10 +640,27 @@ inline dim3 row_block(int nz) {
 #define QUASI_EW(kern, ...) kern<<<ew_grid(kern, 256), 256, 0, s>>>(__VA_ARGS__)
 
 // One time step, enqueued on `s` (captured into a CUDA graph by the caller).
+// Independent transforms (the inverse transforms of psi^ and rho^, the three
+// stress transforms, the five after the projection) are split over s and a
+// second stream s2 between a fork and a join (ev[2i], ev[2i+1]), so that in
+// the captured graph one persistent pass kernel's last tiles overlap the next
+// one's first loads.  s2 == nullptr: everything on s.
 template <typename T>
-cudaError_t enqueue_step(const StepCtx<T>& c, const AxisTables<T>& tb, int* nloop_dev, cudaStream_t s) {
+cudaError_t enqueue_step(const StepCtx<T>& c, const AxisTables<T>& tb, int* nloop_dev, cudaStream_t s,
+                         cudaStream_t s2 = nullptr, const cudaEvent_t* ev = nullptr) {
   const Geom g = c.g;
   const size_t n = size_t(g.nx) * g.ny * g.nz;
+  const cudaStream_t sb = s2 ? s2 : s;
+  auto fork = [&](int i) -> cudaError_t {
+    if (!s2) return cudaSuccess;
+    cudaError_t e = cudaEventRecord(ev[2 * i], s);
+    return e != cudaSuccess ? e : cudaStreamWaitEvent(s2, ev[2 * i], 0);
+  };
+  auto join = [&](int i) -> cudaError_t {
+    if (!s2) return cudaSuccess;
+    cudaError_t e = cudaEventRecord(ev[2 * i + 1], s2);
+    return e != cudaSuccess ? e : cudaStreamWaitEvent(s, ev[2 * i + 1], 0);
+  };
   bump_counter_kernel<<<1, 1, 0, s>>>(nloop_dev);
   QUASI_TRY(cudaGetLastError());
   auto st = [&](T* d) { return StoreField<T>{g, d}; };
@@ -651,14 +668,16 @@ cudaError_t enqueue_step(const StepCtx<T>& c, const AxisTables<T>& tb, int* nloo
   if (c.variant == kQuasi) {
     // a3 prologue quasi.cpp:1036-1057
     // (pairs that share the source, kinds and shift take one dual x pass)
+    QUASI_TRY(fork(0));
     QUASI_TRY(inverse3_mul2(g, tb, kiCT, c.psiq, MDf<T>{c}, MLap<T>{c}, 0, 0, 0, c.df, c.lap, s));
     // a4 gradients quasi.cpp:1120-1232: grad psi with grad lap grad psi, grad rho
-    QUASI_TRY(inverse3_mul2(g, tb, kiSTx, c.psiq, MGrad<T, 0, false>{c}, MGrad<T, 0, true>{c}, 1, 0, 0, c.gx, c.ldx, s));
+    QUASI_TRY(inverse3_mul2(g, tb, kiSTx, c.psiq, MGrad<T, 0, false>{c}, MGrad<T, 0, true>{c}, 1, 0, 0, c.gx, c.ldx, sb));
     QUASI_TRY(inverse3_mul2(g, tb, kiSTy, c.psiq, MGrad<T, 1, false>{c}, MGrad<T, 1, true>{c}, 0, 1, 0, c.gy, c.ldy, s));
-    QUASI_TRY(inverse3_mul2(g, tb, kiSTz, c.psiq, MGrad<T, 2, false>{c}, MGrad<T, 2, true>{c}, 0, 0, 1, c.gz, c.ldz, s));
+    QUASI_TRY(inverse3_mul2(g, tb, kiSTz, c.psiq, MGrad<T, 2, false>{c}, MGrad<T, 2, true>{c}, 0, 0, 1, c.gz, c.ldz, sb));
     QUASI_TRY(inverse3_mul(g, tb, kiSTx, c.rhoq, MGrad<T, 0, false>{c}, 1, 0, 0, st(c.rdx), c.rdx, s));
-    QUASI_TRY(inverse3_mul(g, tb, kiSTy, c.rhoq, MGrad<T, 1, false>{c}, 0, 1, 0, st(c.rdy), c.rdy, s));
+    QUASI_TRY(inverse3_mul(g, tb, kiSTy, c.rhoq, MGrad<T, 1, false>{c}, 0, 1, 0, st(c.rdy), c.rdy, sb));
     QUASI_TRY(inverse3_mul(g, tb, kiSTz, c.rhoq, MGrad<T, 2, false>{c}, 0, 0, 1, st(c.rdz), c.rdz, s));
+    QUASI_TRY(join(0));
     // a5 density + filter quasi.cpp:1237-1268 (rho doubles as the scratch)
     QUASI_EW(rho_law_kernel<T>, c, n);
     QUASI_TRY(cudaGetLastError());
@@ -670,18 +689,22 @@ cudaError_t enqueue_step(const StepCtx<T>& c, const AxisTables<T>& tb, int* nloo
     QUASI_TRY(forward3(g, tb, kCT, ld(c.divv), c.divvq, st(c.divvq), s));
   } else {
     // quasi-stb.cpp:1005-1038 (the unused dRho transform is elided)
+    QUASI_TRY(fork(0));
     QUASI_TRY(inverse3_mul(g, tb, kiCT, c.psiq, MSh<T>{c}, 0, 0, 0, st(c.sh), c.sh, s));
-    QUASI_TRY(inverse3_mul(g, tb, kiSTx, c.psiq, MGrad<T, 0, false>{c}, 1, 0, 0, st(c.gx), c.gx, s));
+    QUASI_TRY(inverse3_mul(g, tb, kiSTx, c.psiq, MGrad<T, 0, false>{c}, 1, 0, 0, st(c.gx), c.gx, sb));
     QUASI_TRY(inverse3_mul(g, tb, kiSTy, c.psiq, MGrad<T, 1, false>{c}, 0, 1, 0, st(c.gy), c.gy, s));
-    QUASI_TRY(inverse3_mul(g, tb, kiSTz, c.psiq, MGrad<T, 2, false>{c}, 0, 0, 1, st(c.gz), c.gz, s));
+    QUASI_TRY(inverse3_mul(g, tb, kiSTz, c.psiq, MGrad<T, 2, false>{c}, 0, 0, 1, st(c.gz), c.gz, sb));
+    QUASI_TRY(join(0));
     // rho == 1, divv == 0, grad rho == 0 (rhoq never leaves 0): quasi-stb.cpp:1232
   }
   // a7 stress quasi.cpp:1298-1330
   QUASI_EW(stress_kernel<T>, c, n);
   QUASI_TRY(cudaGetLastError());
+  QUASI_TRY(fork(1));
   QUASI_TRY(forward3(g, tb, kSTx, ld(c.Sx), c.Sx, st(c.Sx), s));
-  QUASI_TRY(forward3(g, tb, kSTy, ld(c.Sy), c.Sy, st(c.Sy), s));
+  QUASI_TRY(forward3(g, tb, kSTy, ld(c.Sy), c.Sy, st(c.Sy), sb));
   QUASI_TRY(forward3(g, tb, kSTz, ld(c.Sz), c.Sz, st(c.Sz), s));
+  QUASI_TRY(join(1));
   // a8 pressure, a9 velocity, a10 scaled divv quasi.cpp:1336-1900
   {
     const dim3 blk = row_block<T>(g.nz);
@@ -692,11 +715,13 @@ cudaError_t enqueue_step(const StepCtx<T>& c, const AxisTables<T>& tb, int* nloo
     project_kernel<T><<<per_sm * tma_config().sms, blk, 0, s>>>(c);
   }
   QUASI_TRY(cudaGetLastError());
+  QUASI_TRY(fork(2));
   if (c.variant == kQuasi) QUASI_TRY(inverse3(g, tb, kiCT, ld(c.p), c.p, st(c.p), s));
-  QUASI_TRY(inverse3(g, tb, kiSTx, ld(c.vx), c.vx, st(c.vx), s));
+  QUASI_TRY(inverse3(g, tb, kiSTx, ld(c.vx), c.vx, st(c.vx), sb));
   QUASI_TRY(inverse3(g, tb, kiSTy, ld(c.vy), c.vy, st(c.vy), s));
-  QUASI_TRY(inverse3(g, tb, kiSTz, ld(c.vz), c.vz, st(c.vz), s));
+  QUASI_TRY(inverse3(g, tb, kiSTz, ld(c.vz), c.vz, st(c.vz), sb));
   if (c.variant == kQuasi) QUASI_TRY(inverse3(g, tb, kiCT, ld(c.divv), c.divv, st(c.divv), s));
+  QUASI_TRY(join(2));
   // a11 nonlinear term quasi.cpp:1905-1939
   QUASI_EW(nonlinear_kernel<T>, c, n);
   QUASI_TRY(cudaGetLastError());
