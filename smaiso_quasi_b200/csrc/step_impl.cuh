@@ -638,11 +638,13 @@ inline dim3 row_block(int nz) {
   return dim3(tx, ty);
 }
 #define QUASI_EW(kern, ...) kern<<<ew_grid(kern, 256), 256, 0, s>>>(__VA_ARGS__)
+#define QUASI_EW_ON(kern, strm, ...) kern<<<ew_grid(kern, 256), 256, 0, strm>>>(__VA_ARGS__)
 
 // One time step, enqueued on `s` (captured into a CUDA graph by the caller).
 // Independent transforms (the inverse transforms of psi^ and rho^, the three
 // stress transforms, the five after the projection) are split over s and a
-// second stream s2 between a fork and a join (ev[2i], ev[2i+1]), so that in
+// second stream s2 between a fork and a join (ev[2i], ev[2i+1]; ev[6] orders
+// the second stream's stress transform after the stress kernel), so that in
 // the captured graph one persistent pass kernel's last tiles overlap the next
 // one's first loads.  s2 == nullptr: everything on s.
 template <typename T>
@@ -683,10 +685,7 @@ cudaError_t enqueue_step(const StepCtx<T>& c, const AxisTables<T>& tb, int* nloo
     QUASI_TRY(cudaGetLastError());
     QUASI_TRY(forward3(g, tb, kCT, ld(c.rho), c.rho, StRhoq<T>{c}, s));
     QUASI_TRY(inverse3(g, tb, kiCT, ld(c.rhoq), c.rho, st(c.rho), s));
-    // a6 divv quasi.cpp:1273-1293
-    QUASI_EW(divv_kernel<T>, c, n);
-    QUASI_TRY(cudaGetLastError());
-    QUASI_TRY(forward3(g, tb, kCT, ld(c.divv), c.divvq, st(c.divvq), s));
+
   } else {
     // quasi-stb.cpp:1005-1038 (the unused dRho transform is elided)
     QUASI_TRY(fork(0));
@@ -697,12 +696,23 @@ cudaError_t enqueue_step(const StepCtx<T>& c, const AxisTables<T>& tb, int* nloo
     QUASI_TRY(join(0));
     // rho == 1, divv == 0, grad rho == 0 (rhoq never leaves 0): quasi-stb.cpp:1232
   }
-  // a7 stress quasi.cpp:1298-1330
+  // a6 divv quasi.cpp:1273-1293 on the second stream, beside a7 the stress
+  // quasi.cpp:1298-1330 (neither reads what the other writes; the projection
+  // after the join reads both)
+  QUASI_TRY(fork(1));
+  if (c.variant == kQuasi) {
+    QUASI_EW_ON(divv_kernel<T>, sb, c, n);
+    QUASI_TRY(cudaGetLastError());
+    QUASI_TRY(forward3(g, tb, kCT, ld(c.divv), c.divvq, st(c.divvq), sb));
+  }
   QUASI_EW(stress_kernel<T>, c, n);
   QUASI_TRY(cudaGetLastError());
-  QUASI_TRY(fork(1));
-  QUASI_TRY(forward3(g, tb, kSTx, ld(c.Sx), c.Sx, st(c.Sx), s));
+  if (s2) {   // Sy on the second stream once the stress is written
+    QUASI_TRY(cudaEventRecord(ev[6], s));
+    QUASI_TRY(cudaStreamWaitEvent(s2, ev[6], 0));
+  }
   QUASI_TRY(forward3(g, tb, kSTy, ld(c.Sy), c.Sy, st(c.Sy), sb));
+  QUASI_TRY(forward3(g, tb, kSTx, ld(c.Sx), c.Sx, st(c.Sx), s));
   QUASI_TRY(forward3(g, tb, kSTz, ld(c.Sz), c.Sz, st(c.Sz), s));
   QUASI_TRY(join(1));
   // a8 pressure, a9 velocity, a10 scaled divv quasi.cpp:1336-1900
