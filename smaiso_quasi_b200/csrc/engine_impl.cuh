@@ -476,7 +476,7 @@ class Engine : public EngineBase {
   int* nloop_dev_ = nullptr;
   double* partial_ = nullptr;
   cudaStream_t stream2_ = nullptr;
-  cudaEvent_t fork_ev_[7] = {};
+  cudaEvent_t fork_ev_[8] = {};
   int* tma_err_ = nullptr;
   int sms_ = 148;
   bool fused_yz_ = false;

@@ -644,7 +644,8 @@ inline dim3 row_block(int nz) {
 // Independent transforms (the inverse transforms of psi^ and rho^, the three
 // stress transforms, the five after the projection) are split over s and a
 // second stream s2 between a fork and a join (ev[2i], ev[2i+1]; ev[6] orders
-// the second stream's stress transform after the stress kernel), so that in
+// the second stream's stress transform after the stress kernel, ev[7] the
+// density chain after the gradients), so that in
 // the captured graph one persistent pass kernel's last tiles overlap the next
 // one's first loads.  s2 == nullptr: everything on s.
 template <typename T>
@@ -670,21 +671,28 @@ cudaError_t enqueue_step(const StepCtx<T>& c, const AxisTables<T>& tb, int* nloo
   if (c.variant == kQuasi) {
     // a3 prologue quasi.cpp:1036-1057
     // (pairs that share the source, kinds and shift take one dual x pass)
-    QUASI_TRY(fork(0));
-    QUASI_TRY(inverse3_mul2(g, tb, kiCT, c.psiq, MDf<T>{c}, MLap<T>{c}, 0, 0, 0, c.df, c.lap, s));
     // a4 gradients quasi.cpp:1120-1232: grad psi with grad lap grad psi, grad rho
-    QUASI_TRY(inverse3_mul2(g, tb, kiSTx, c.psiq, MGrad<T, 0, false>{c}, MGrad<T, 0, true>{c}, 1, 0, 0, c.gx, c.ldx, sb));
-    QUASI_TRY(inverse3_mul2(g, tb, kiSTy, c.psiq, MGrad<T, 1, false>{c}, MGrad<T, 1, true>{c}, 0, 1, 0, c.gy, c.ldy, s));
-    QUASI_TRY(inverse3_mul2(g, tb, kiSTz, c.psiq, MGrad<T, 2, false>{c}, MGrad<T, 2, true>{c}, 0, 0, 1, c.gz, c.ldz, sb));
-    QUASI_TRY(inverse3_mul(g, tb, kiSTx, c.rhoq, MGrad<T, 0, false>{c}, 1, 0, 0, st(c.rdx), c.rdx, s));
-    QUASI_TRY(inverse3_mul(g, tb, kiSTy, c.rhoq, MGrad<T, 1, false>{c}, 0, 1, 0, st(c.rdy), c.rdy, sb));
-    QUASI_TRY(inverse3_mul(g, tb, kiSTz, c.rhoq, MGrad<T, 2, false>{c}, 0, 0, 1, st(c.rdz), c.rdz, s));
-    QUASI_TRY(join(0));
+    QUASI_TRY(fork(0));
+    QUASI_TRY(inverse3_mul2(g, tb, kiSTx, c.psiq, MGrad<T, 0, false>{c}, MGrad<T, 0, true>{c}, 1, 0, 0, c.gx, c.ldx, s));
+    QUASI_TRY(inverse3_mul2(g, tb, kiSTy, c.psiq, MGrad<T, 1, false>{c}, MGrad<T, 1, true>{c}, 0, 1, 0, c.gy, c.ldy, sb));
+    QUASI_TRY(inverse3_mul2(g, tb, kiSTz, c.psiq, MGrad<T, 2, false>{c}, MGrad<T, 2, true>{c}, 0, 0, 1, c.gz, c.ldz, s));
+    QUASI_TRY(inverse3_mul(g, tb, kiSTx, c.rhoq, MGrad<T, 0, false>{c}, 1, 0, 0, st(c.rdx), c.rdx, sb));
+    QUASI_TRY(inverse3_mul(g, tb, kiSTy, c.rhoq, MGrad<T, 1, false>{c}, 0, 1, 0, st(c.rdy), c.rdy, s));
+    QUASI_TRY(inverse3_mul(g, tb, kiSTz, c.rhoq, MGrad<T, 2, false>{c}, 0, 0, 1, st(c.rdz), c.rdz, sb));
+    // the density chain needs grad psi and must not rewrite rho^ before the grad
+    // rho transforms have read it: s waits for the second stream's share ...
+    if (s2) {
+      QUASI_TRY(cudaEventRecord(ev[7], s2));
+      QUASI_TRY(cudaStreamWaitEvent(s, ev[7], 0));
+    }
+    // ... which then runs a3's prologue quasi.cpp:1036-1057 beside it
+    QUASI_TRY(inverse3_mul2(g, tb, kiCT, c.psiq, MDf<T>{c}, MLap<T>{c}, 0, 0, 0, c.df, c.lap, sb));
     // a5 density + filter quasi.cpp:1237-1268 (rho doubles as the scratch)
     QUASI_EW(rho_law_kernel<T>, c, n);
     QUASI_TRY(cudaGetLastError());
     QUASI_TRY(forward3(g, tb, kCT, ld(c.rho), c.rho, StRhoq<T>{c}, s));
     QUASI_TRY(inverse3(g, tb, kiCT, ld(c.rhoq), c.rho, st(c.rho), s));
+    QUASI_TRY(join(0));
 
   } else {
     // quasi-stb.cpp:1005-1038 (the unused dRho transform is elided)
