@@ -85,8 +85,15 @@ struct ScaleStore {
   Geom g;
   T* dst;
   T s;
-  __device__ void operator()(int i, int j, int k, T v) const { dst[lin(g, i, j, k)] = v * s; }
+  __device__ T value(int, int, int, T v) const { return v * s; }
+  __host__ __device__ T* stage_dst() const { return dst; }
+  __device__ void operator()(int i, int j, int k, T v) const { dst[lin(g, i, j, k)] = value(i, j, k, v); }
 };
+
+// Storers that map a value before it lands (value(i, j, k, v)) in one field
+// (stage_dst()): their x / y tiles can be staged and TMA-stored as well.
+template <class S, class = void> struct HasStageValue : std::false_type {};
+template <class S> struct HasStageValue<S, std::void_t<decltype(&S::stage_dst)>> : std::true_type {};
 
 
 template <int AXIS>
@@ -269,6 +276,23 @@ struct RowStageSnk {
   }
 };
 
+// The same for a storer with value(i, j, k, v): the mapped values are staged.
+template <typename T, int AXIS, class Store>
+struct RowStageValSnk {
+  static constexpr bool kAliasesTile = true;
+  T* stg;
+  int P, outer, k0;
+  Store st;
+  __device__ void put(int g, int n, T a, T b) const {
+    const int k = k0 + 2 * g;
+    const int i = AXIS == 1 ? outer : n, j = AXIS == 1 ? n : outer;
+    typename Vec2<T>::type v;
+    v.x = st.value(i, j, k, a);
+    v.y = st.value(i, j, k + 1, b);
+    *reinterpret_cast<typename Vec2<T>::type*>(stg + n * P + 2 * g) = v;
+  }
+};
+
 // Identity multiplier (plain passes).
 struct NoMul {
   static constexpr bool kActive = false;
@@ -385,6 +409,7 @@ __global__ void __launch_bounds__(tma_threads<T>(), tma_min_blocks<IP>())
   static_assert(!TSTORE || (!IP && AXIS != 2), "TMA-stored tiles are x / y passes with a work tile");
   static_assert(!IP || AXIS != 2, "in-place raw tiles are for x / y passes");
   constexpr bool kDual = !std::is_same<Mul2, NoMul>::value;
+  static_assert(!TSTORE || !kDual || IsStoreField<Store>::value, "dual passes stage plain fields");
   static_assert(tma_threads<T>() % (P / 2) == 0, "MulSrc::prep: each thread reads one pencil pair");
   static_assert(!kDual || (!IP && AXIS != 2), "dual tiles are x / y passes with a work tile");
   constexpr int NT = tma_threads<T>();
@@ -498,9 +523,13 @@ __global__ void __launch_bounds__(tma_threads<T>(), tma_min_blocks<IP>())
       const int outer = t / kt, k0 = (t - outer * kt) * P;
       MulSrc<T, AXIS, Mul> src{raw, P, outer, k0, mul};
       src.prep(tid % (P / 2));
-      if constexpr (TSTORE) {
+      if constexpr (TSTORE && IsStoreField<Store>::value) {
         r2r_tile<T, N, P / 2, NT, false>(ex, tid, kind, reinterpret_cast<Cx<T>*>(work), src,
                                           RowStageSnk<T>{work, P}, tb, issue_next);
+        store_tile(&dmap);
+      } else if constexpr (TSTORE) {
+        r2r_tile<T, N, P / 2, NT, false>(ex, tid, kind, reinterpret_cast<Cx<T>*>(work), src,
+                                          RowStageValSnk<T, AXIS, Store>{work, P, outer, k0, st}, tb, issue_next);
         store_tile(&dmap);
       } else {
         r2r_tile<T, N, P / 2, NT, false>(ex, tid, kind, reinterpret_cast<Cx<T>*>(work), src,
@@ -612,10 +641,14 @@ cudaError_t launch_tma_pass(const Geom& g, int kind, Tables<T> tb, const T* src,
   CUtensorMap map;
   if (!MapCache::get().lookup(&map, src, int(sizeof(T)), g.nx, g.ny, g.nz, AXIS, box)) return cudaErrorNotSupported;
   // plain field outputs of x / y passes leave through TMA stores (same box)
-  constexpr bool TSTORE = IsStoreField<Store>::value && AXIS != 2 && !IP;
+  constexpr bool kStaged = IsStoreField<Store>::value || HasStageValue<Store>::value;
+  constexpr bool TSTORE = kStaged && AXIS != 2 && !IP;
   CUtensorMap dmap = map, dmap2 = map;
   if constexpr (TSTORE) {
-    if (!MapCache::get().lookup(&dmap, st.dst, int(sizeof(T)), g.nx, g.ny, g.nz, AXIS, box))
+    const T* dptr;
+    if constexpr (IsStoreField<Store>::value) dptr = st.dst;
+    else dptr = st.stage_dst();
+    if (!MapCache::get().lookup(&dmap, dptr, int(sizeof(T)), g.nx, g.ny, g.nz, AXIS, box))
       return cudaErrorNotSupported;
     if constexpr (!std::is_same<Mul2, NoMul>::value) {
       if (!MapCache::get().lookup(&dmap2, st2.dst, int(sizeof(T)), g.nx, g.ny, g.nz, AXIS, box))

@@ -154,6 +154,7 @@ template <typename T> struct StRhoq {
   __device__ T value(int i, int j, int k, T v) const {
     return T(c.scale * double(v) * (__ldg(c.fx + i) * __ldg(c.fy + j) * __ldg(c.fz + k)));
   }
+  __host__ __device__ T* stage_dst() const { return c.rhoq; }
   __device__ void operator()(int i, int j, int k, T v) const { c.rhoq[at(c, i, j, k)] = value(i, j, k, v); }
   __device__ void pair(int i, int j, int k, T a, T b) const {
     typename Vec2<T>::type v;
