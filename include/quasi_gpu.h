@@ -168,7 +168,11 @@ QUASI_API int quasi_load(quasi_handle* h, const char* path);
  * library keeps until exit, so grids are limited to 2^25 cells (larger ones
  * are rejected).  The first call on a device looks that array up; make it
  * before any stream capture.  Calls that overlap on the GPU race.
- * df may be NULL for the quasi-stb variant (no energy). */
+ * The call runs on cfg->device (the caller's current device is restored),
+ * rejects field pointers that are not device memory of that device
+ * (QUASI_ERR_INVALID), and waits for its stream, so it must not be made on
+ * a stream that is being captured (QUASI_ERR_STATE).  dt, q0 and nw must be
+ * positive.  df may be NULL for the quasi-stb variant (no energy; out[2] = 0). */
 QUASI_API int quasi_diagnostics_noalloc(const quasi_config* cfg, const void* psi, const void* psi_old,
                                         const void* rho, const void* df, double out[3], void* stream);
 

@@ -50,6 +50,49 @@ def test_noalloc_matches_handle_on_two_calls(precision, dtype):
         np.testing.assert_allclose(np.array(out), ref, rtol=RTOL)
 
 
+def test_noalloc_stb_without_df():
+    """quasi-stb has no energy: df may be NULL and out[2] is 0."""
+    import torch
+    q, fn = _entry()
+    cfg = q.default_config("stb", 16, 16, 32)
+    sim = q.Simulation(cfg)
+    sim.set_psi(q.initial_condition(cfg, "stb", seed=4))
+    sim.init()
+    for before in (1, 3):
+        sim.step(before)
+        prev = sim.field("psi")
+        sim.step(1)
+        ref = np.array(sim.diagnostics())
+        dev = [torch.from_numpy(a).to("cuda") for a in (sim.field("psi"), prev, sim.field("rho"))]
+        torch.cuda.synchronize()
+        out = (ctypes.c_double * 3)(7.0, 7.0, 7.0)
+        rc = fn(ctypes.byref(cfg), *[ctypes.c_void_p(t.data_ptr()) for t in dev], None, out, None)
+        assert rc == 0, q.lib().quasi_last_error().decode()
+        np.testing.assert_allclose(np.array(out)[:2], ref[:2], rtol=RTOL)
+        assert out[2] == 0.0
+
+
+def test_noalloc_rejects_host_pointers():
+    """Fields in host memory are refused before anything is launched."""
+    q, fn = _entry()
+    cfg = q.default_config("quasi", 16, 16, 32)
+    host = [np.zeros((16, 16, 32)) for _ in range(4)]
+    out = (ctypes.c_double * 3)()
+    rc = fn(ctypes.byref(cfg), *[ctypes.c_void_p(a.ctypes.data) for a in host], out, None)
+    assert rc == -1
+    assert b"not device memory" in q.lib().quasi_last_error()
+
+
+def test_noalloc_rejects_nonpositive_dt():
+    q, fn = _entry()
+    cfg = q.default_config("quasi", 16, 16, 32)
+    cfg.dt = 0.0
+    out = (ctypes.c_double * 3)()
+    dummy = ctypes.c_void_p(16)                       # never dereferenced: rejected first
+    rc = fn(ctypes.byref(cfg), dummy, dummy, dummy, dummy, out, None)
+    assert rc == -1
+
+
 def test_noalloc_rejects_grids_beyond_its_scratch():
     q, fn = _entry()
     cfg = q.default_config("quasi", 512, 512, 256)   # 2^26 cells > 2^25
