@@ -15,15 +15,17 @@
 #   3. the loop bound (L1 > 1e-6 / loopLim)                -> also nLoop < QUASI_MAXSTEPS
 #   4. stepL1 / stepSave                                   -> QUASI_STEPL1 / QUASI_STEPSAVE
 #   5. text dump precision (ostream default: 6 digits)     -> 17 significant digits
-# Usage: oracle/build_ref.sh [reference_root]   (default /root/reference)
+# Usage: oracle/build_ref.sh [reference_root]   (default: $QUASI_REFERENCE, else the
+# reference checkout of the build container, /root/reference); exit code 3 when
+# the sources are absent (the GPU box uses the prebuilt oracle/_ref)
 set -euo pipefail
 REF="${1:-${QUASI_REFERENCE:-/root/reference}}"
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
 OUT="$HERE/_ref"
 CXX="${CXX:-g++}"
 if [ ! -f "$REF/quasi/quasi.cpp" ]; then
-  echo "build_ref: reference sources not found under $REF" >&2
-  exit 1
+  echo "build_ref: reference sources not found under $REF (set QUASI_REFERENCE)" >&2
+  exit 3
 fi
 mkdir -p "$OUT"
 

@@ -59,14 +59,6 @@ inline void host_parallel(size_t n, F&& f) {
   for (auto& th : pool) th.join();
 }
 
-// QUASI_FUSED_YZ=1 selects the one-pass y+z cluster kernel (yz_plane.cuh)
-// for the plane shapes it covers; by default the y and z passes run as two
-// TMA passes, which measured faster on B200.
-inline bool fused_yz_requested() {
-  const char* v = std::getenv("QUASI_FUSED_YZ");
-  return v && v[0] == '1';
-}
-
 // Validates a configuration; returns an empty string when it is usable.
 std::string validate_config(const quasi_config& c);
 

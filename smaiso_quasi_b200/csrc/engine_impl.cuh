@@ -110,7 +110,6 @@ class Engine : public EngineBase {
       return QUASI_ERR_CUDA;
     if (!cuda_ok(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, cfg_.device), "attribute"))
       return QUASI_ERR_CUDA;
-    fused_yz_ = fused_yz_requested();
     if (!cuda_ok(cudaMallocHost(&host_stage_, n_ * sizeof(T) + 64), "host alloc")) return QUASI_ERR_NOMEM;
     // wavenumber tables, quasi.cpp:397-431
     const int len[3] = {g_.nx, g_.ny, g_.nz};
@@ -363,7 +362,6 @@ class Engine : public EngineBase {
     t.err = tma_err_;
     t.sms = sms_;
     t.enabled = true;
-    t.yz = fused_yz_;
   }
 
   bool cuda_ok(cudaError_t e, const char* what) {
@@ -479,7 +477,6 @@ class Engine : public EngineBase {
   cudaEvent_t fork_ev_[8] = {};
   int* tma_err_ = nullptr;
   int sms_ = 148;
-  bool fused_yz_ = false;
   void* host_stage_ = nullptr;
   DevTwiddles<T> tw_[3];
   AxisTables<T> tb_{};

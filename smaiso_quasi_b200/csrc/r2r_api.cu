@@ -22,7 +22,6 @@ struct R2RBase {
     t.err = tma_err;
     t.sms = sms;
     t.enabled = true;
-    t.yz = fused_yz_requested();
   }
 };
 

@@ -218,17 +218,11 @@ struct SmemSnk {
   }
 };
 
-// Tile layouts between stages: complex element e of pencil g at
-// cb[g * GS + e * ES].  The default is pencil-major with the odd stride
-// LD = N + 1; element-major (GS = 1, ES = G) is the layout a TMA box of G
-// complex columns lands in, conflict-free for 64-bit accesses when G = 16.
+// Tile layout between stages: complex element e of pencil g at
+// cb[g * GS + e * ES], pencil-major with the odd stride LD = N + 1.
 template <int N>
 struct PencilMajor {
   static constexpr int GS = tile_ld(N), ES = 1;
-};
-template <int G>
-struct ElemMajor {
-  static constexpr int GS = 1, ES = G;
 };
 
 template <typename T, int N, int G, int NT, class L = PencilMajor<N>>

@@ -341,13 +341,6 @@ struct MulSrc {
 
 constexpr uint32_t kTmaPollLimit = 1u << 24;
 
-// Axes (bit 0: x, bit 1: y) whose TMA passes transform in place in the
-// landing buffer (see tma_pass_kernel's IP).
-#ifndef QUASI_TMA_INPLACE
-#define QUASI_TMA_INPLACE 0
-#endif
-template <int AXIS> constexpr bool tma_in_place() { return AXIS != 2 && ((QUASI_TMA_INPLACE >> AXIS) & 1); }
-
 template <int AXIS, int P>
 __device__ __forceinline__ void tile_origin(const Geom& g, int tile, int& c0, int& c1, int& c2) {
   if (AXIS == 2) {   // P rows (i, j0..j0+P-1); P divides ny
@@ -384,41 +377,32 @@ __device__ __forceinline__ void tma_issue_tile(const CUtensorMap* map, T* raw, u
 
 template <typename T> constexpr int tma_threads() { return 256; }
 
-// IP (x / y only): the tile is transformed in place in its raw buffer, whose
-// [n][P] layout is the element-major complex layout [n][P/2]; no padded work
-// tile, so three CTAs fit an SM.  The raw buffer is then recycled only after
-// the tile's last read.
-template <typename T, int N, int AXIS, int P, bool IP> constexpr int tma_work_elems() {
-  return IP ? 0 : ((P * tile_ld(N) + 15) / 16) * 16;
-}
-template <bool IP> constexpr int tma_min_blocks() { return IP ? 3 : 2; }
+template <typename T, int N, int P> constexpr int tma_work_elems() { return ((P * tile_ld(N) + 15) / 16) * 16; }
 
-// Mul2 != NoMul (x / y, not IP): each tile, loaded once, is transformed twice,
+// Mul2 != NoMul (x / y): each tile, loaded once, is transformed twice,
 // with mul into st and with mul2 into st2 (two inverse transforms of the same
 // spectral field that differ only in their multiplier).
-// TSTORE (plain field outputs, not IP): the last stage writes the staging rows
+// TSTORE (plain field outputs): the last stage writes the staging rows
 // over the work tile and one thread stores the tile through dmap (dmap2 for
 // the dual pass's second output); the next tile's first stage waits for the
 // store to have read them.
-template <typename T, int N, int AXIS, int P, class Store, class Mul, bool IP = false, class Mul2 = NoMul,
-          bool TSTORE = false>
-__global__ void __launch_bounds__(tma_threads<T>(), tma_min_blocks<IP>())
+template <typename T, int N, int AXIS, int P, class Store, class Mul, class Mul2 = NoMul, bool TSTORE = false>
+__global__ void __launch_bounds__(tma_threads<T>(), 2)
     tma_pass_kernel(const __grid_constant__ CUtensorMap map, Geom g, int kind, Tables<T> tb, Store st, int ntiles,
                     int* err, Mul mul, int dc1, int dc2, int ks, Store st2, Mul2 mul2,
                     const __grid_constant__ CUtensorMap dmap, const __grid_constant__ CUtensorMap dmap2) {
-  static_assert(!TSTORE || (!IP && AXIS != 2), "TMA-stored tiles are x / y passes with a work tile");
-  static_assert(!IP || AXIS != 2, "in-place raw tiles are for x / y passes");
+  static_assert(!TSTORE || AXIS != 2, "TMA-stored tiles are x / y passes");
   constexpr bool kDual = !std::is_same<Mul2, NoMul>::value;
   static_assert(!TSTORE || !kDual || IsStoreField<Store>::value, "dual passes stage plain fields");
   static_assert(tma_threads<T>() % (P / 2) == 0, "MulSrc::prep: each thread reads one pencil pair");
-  static_assert(!kDual || (!IP && AXIS != 2), "dual tiles are x / y passes with a work tile");
+  static_assert(!kDual || AXIS != 2, "dual tiles are x / y passes");
   constexpr int NT = tma_threads<T>();
   constexpr int LD = tile_ld(N);
   extern __shared__ __align__(128) unsigned char smem_raw[];
   T* raw0 = reinterpret_cast<T*>(smem_raw);
   T* raw1 = raw0 + P * N;
   T* work = raw1 + P * N;
-  uint64_t* bar = reinterpret_cast<uint64_t*>(work + tma_work_elems<T, N, AXIS, P, IP>());
+  uint64_t* bar = reinterpret_cast<uint64_t*>(work + tma_work_elems<T, N, P>());
   const int tid = threadIdx.x;
   {
     // per-CTA shared-memory copies of the twiddle tables (N entries each)
@@ -482,18 +466,7 @@ __global__ void __launch_bounds__(tma_threads<T>(), tma_min_blocks<IP>())
         tma_issue_tile<T, N, AXIS, P>(&map, raw, &bar[b], g, t_next, dc1, dc2);
       }
     };
-    if constexpr (AXIS != 2 && IP) {
-      const int kt = g.nz / P;
-      const int outer = t / kt, k0 = (t - outer * kt) * P;
-      MulSrc<T, AXIS, Mul, true> src{raw, P, outer, k0, mul};
-      src.prep(tid % (P / 2));
-      r2r_tile<T, N, P / 2, NT, false, ElemMajor<P / 2>>(ex, tid, kind, reinterpret_cast<Cx<T>*>(raw), src,
-                                                          GlobSnk<T, AXIS, Store>{st, outer, k0}, tb);
-      fence_proxy_async_smem();   // this thread's writes to raw precede the copy that refills it
-      __syncthreads();            // the last read of this raw buffer is done
-      issue_next();
-      continue;
-    } else if constexpr (AXIS != 2 && kDual) {
+    if constexpr (AXIS != 2 && kDual) {
       const int kt = g.nz / P;
       const int outer = t / kt, k0 = (t - outer * kt) * P;
       MulSrc<T, AXIS, Mul> src{raw, P, outer, k0, mul};
@@ -581,9 +554,9 @@ __global__ void __launch_bounds__(tma_threads<T>(), tma_min_blocks<IP>())
   }
 }
 
-template <typename T, int N, int AXIS, int P, bool IP>
+template <typename T, int N, int P>
 inline size_t tma_smem_bytes() {
-  return size_t(2) * P * N * sizeof(T) + size_t(tma_work_elems<T, N, AXIS, P, IP>()) * sizeof(T) + 16 +
+  return size_t(2) * P * N * sizeof(T) + size_t(tma_work_elems<T, N, P>()) * sizeof(T) + 16 +
          2 * N * sizeof(Cx<T>);
 }
 
@@ -621,15 +594,13 @@ struct TmaConfig {
   int* err = nullptr;     // device flag, nonzero after a timed-out wait
   int sms = 148;          // CTAs per SM x SMs bounds the persistent grid
   bool enabled = true;
-  bool yz = false;        // fuse the y and z passes into one cluster pass
 };
 inline TmaConfig& tma_config() {
   static thread_local TmaConfig c;
   return c;
 }
 
-template <typename T, int N, int AXIS, int P, class Store, class Mul = NoMul, class Mul2 = NoMul,
-          bool IP = tma_in_place<AXIS>() && std::is_same<Mul2, NoMul>::value>
+template <typename T, int N, int AXIS, int P, class Store, class Mul = NoMul, class Mul2 = NoMul>
 cudaError_t launch_tma_pass(const Geom& g, int kind, Tables<T> tb, const T* src, Store st, cudaStream_t s,
                             Mul mul = Mul(), int dc1 = 0, int dc2 = 0, int ks = 0, Store st2 = Store(),
                             Mul2 mul2 = Mul2()) {
@@ -642,7 +613,7 @@ cudaError_t launch_tma_pass(const Geom& g, int kind, Tables<T> tb, const T* src,
   if (!MapCache::get().lookup(&map, src, int(sizeof(T)), g.nx, g.ny, g.nz, AXIS, box)) return cudaErrorNotSupported;
   // plain field outputs of x / y passes leave through TMA stores (same box)
   constexpr bool kStaged = IsStoreField<Store>::value || HasStageValue<Store>::value;
-  constexpr bool TSTORE = kStaged && AXIS != 2 && !IP;
+  constexpr bool TSTORE = kStaged && AXIS != 2;
   CUtensorMap dmap = map, dmap2 = map;
   if constexpr (TSTORE) {
     const T* dptr;
@@ -655,8 +626,8 @@ cudaError_t launch_tma_pass(const Geom& g, int kind, Tables<T> tb, const T* src,
         return cudaErrorNotSupported;
     }
   }
-  const size_t smem = tma_smem_bytes<T, N, AXIS, P, IP>();
-  auto kern = tma_pass_kernel<T, N, AXIS, P, Store, Mul, IP, Mul2, TSTORE>;
+  const size_t smem = tma_smem_bytes<T, N, P>();
+  auto kern = tma_pass_kernel<T, N, AXIS, P, Store, Mul, Mul2, TSTORE>;
   static int per_sm = 0;   // per instantiation: resident CTAs per SM
   if (per_sm == 0) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -12,7 +12,6 @@
 #include <cuda_runtime.h>
 
 #include "r2r_pass.cuh"
-#include "yz_plane.cuh"
 #include "z_pass.cuh"
 
 namespace quasi {
@@ -520,19 +519,13 @@ struct AxisTables {
   Tables<T> t[3];
 };
 
-// y and z passes of `src` (plain field) into `st`: one cluster pass when the
-// plane shape allows it, else two passes (the second in place on st.dst).
-// kshift = 1: the z pass transforms row[k + 1] (zero at the top) in place of
-// row[k], the z shift of a z gradient (quasi.cpp:1163-1186).
+// y and z passes of `src` (plain field) into `st` (the y pass in place, the
+// z pass into st.dst).  kshift = 1: the z pass transforms row[k + 1] (zero at
+// the top) in place of row[k], the z shift of a z gradient
+// (quasi.cpp:1163-1186).
 template <typename T, class Store>
 cudaError_t yz3(const Geom& g, const AxisTables<T>& tb, const int kinds[3], T* src, Store st, cudaStream_t s,
                 int kshift = 0) {
-  if constexpr (IsStoreField<Store>::value) {
-    if (!kshift) {
-      cudaError_t e = launch_yz<T>(g, kinds[1], kinds[2], tb.t[1], tb.t[2], src, st.dst, s);
-      if (e != cudaErrorNotSupported) return e;
-    }
-  }
   cudaError_t e;
   if ((e = launch_pass<T, 1>(g, kinds[1], tb.t[1], LoadField<T>{g, src}, StoreField<T>{g, src}, s)) != cudaSuccess)
     return e;
@@ -563,28 +556,16 @@ cudaError_t inverse3_mul(const Geom& g, const AxisTables<T>& tb, const int kinds
   return yz3(g, tb, kinds, dst, StoreField<T>{g, dst}, s, dk);
 }
 
-// Forward: z and y (loader -> dst), then x pass (storer).  A plain field
-// loader takes the fused cluster pass.
+// Forward: z and y (loader -> dst), then x pass (storer).
 template <typename T, class Load, class Store>
 cudaError_t forward3(const Geom& g, const AxisTables<T>& tb, const int kinds[3], Load ld, T* dst, Store st,
                      cudaStream_t s) {
-  cudaError_t e;
-  bool fused = false;
-  if constexpr (std::is_same<Load, LoadField<T>>::value) {
-    e = launch_yz<T>(g, kinds[1], kinds[2], tb.t[1], tb.t[2], ld.src, dst, s);
-    if (e != cudaErrorNotSupported) {
-      if (e != cudaSuccess) return e;
-      fused = true;
-    }
-  }
-  if (!fused) {
-    e = cudaErrorNotSupported;
-    if constexpr (std::is_same<Load, LoadField<T>>::value) e = launch_zpass<T>(g, kinds[2], tb.t[2], ld.src, dst, s);
-    if (e == cudaErrorNotSupported) e = launch_pass<T, 2>(g, kinds[2], tb.t[2], ld, StoreField<T>{g, dst}, s);
-    if (e != cudaSuccess) return e;
-    if ((e = launch_pass<T, 1>(g, kinds[1], tb.t[1], LoadField<T>{g, dst}, StoreField<T>{g, dst}, s)) != cudaSuccess)
-      return e;
-  }
+  cudaError_t e = cudaErrorNotSupported;
+  if constexpr (std::is_same<Load, LoadField<T>>::value) e = launch_zpass<T>(g, kinds[2], tb.t[2], ld.src, dst, s);
+  if (e == cudaErrorNotSupported) e = launch_pass<T, 2>(g, kinds[2], tb.t[2], ld, StoreField<T>{g, dst}, s);
+  if (e != cudaSuccess) return e;
+  if ((e = launch_pass<T, 1>(g, kinds[1], tb.t[1], LoadField<T>{g, dst}, StoreField<T>{g, dst}, s)) != cudaSuccess)
+    return e;
   return launch_pass<T, 0>(g, kinds[0], tb.t[0], LoadField<T>{g, dst}, st, s);
 }
 
