@@ -3,6 +3,7 @@
 #pragma once
 #include <cstdint>
 #include <fstream>
+#include <mutex>
 
 #include "engine.cuh"
 
@@ -14,9 +15,11 @@ namespace quasi {
 constexpr int kDiagBlocks = 592;   // 4 x 148 SMs
 constexpr int kDiagThreads = 256;
 
-template <typename T>
-__global__ void __launch_bounds__(kDiagThreads) diag_partial_kernel(const T* psi, const T* psi_old, const T* rho,
-                                                                    const T* df, double ep, double alpha, double beta,
+// P: the type of psi and psi_old, R: of rho, F: of df (the engine holds psi
+// and rho in double; the allocation-free entry point takes one type for all)
+template <typename P, typename R = P, typename F = P>
+__global__ void __launch_bounds__(kDiagThreads) diag_partial_kernel(const P* psi, const P* psi_old, const R* rho,
+                                                                    const F* df, double ep, double alpha, double beta,
                                                                     double gamma, int with_energy, size_t n,
                                                                     double* partial) {
   double a = 0, b = 0, m = 0, en = 0;
@@ -58,7 +61,11 @@ static __global__ void diag_final_kernel(const double* partial, int nblocks, dou
 template <typename T>
 class Engine : public EngineBase {
  public:
-  static constexpr int kFields = 34;
+  // fields of the storage type (+ the float copies of psiq and rhoq); then
+  // the double fields: psiq x 3, rhoq, rho, rho_old, psi x 2, grad psi x 3
+  // (+ the scratch of the double transforms in the FP32 form)
+  static constexpr int kFields = 20 + (kStateCopy<T> ? 2 : 0);
+  static constexpr int kDFields = 11 + (kStateCopy<T> ? 1 : 0);
   static constexpr int kPhases = 6;   // lcm of the 3-buffer psiq and 2-buffer Nq rotations
 
   explicit Engine(const quasi_config& cfg) : cfg_(cfg) {}
@@ -71,6 +78,11 @@ class Engine : public EngineBase {
       MapCache::get().forget(slab_, static_cast<char*>(slab_) + size_t(kFields) * n_ * sizeof(T));
       cudaFree(slab_);
     }
+    if (dslab_) {
+      MapCache::get().forget(dslab_, dslab_ + size_t(kDFields) * n_);
+      cudaFree(dslab_);
+    }
+    for (auto& t : tw64_) t.release();
     if (tma_err_) cudaFree(tma_err_);
     if (tabs_) cudaFree(tabs_);
     if (nloop_dev_) cudaFree(nloop_dev_);
@@ -96,13 +108,14 @@ class Engine : public EngineBase {
     for (auto& e : fork_ev_)
       if (!cuda_ok(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event")) return QUASI_ERR_CUDA;
     if (!cuda_ok(cudaEventCreate(&ev0_), "event") || !cuda_ok(cudaEventCreate(&ev1_), "event")) return QUASI_ERR_CUDA;
-    const size_t bytes = size_t(kFields) * n_ * sizeof(T);
-    if (cudaMalloc(&slab_, bytes) != cudaSuccess) {
+    const size_t bytes = size_t(kFields) * n_ * sizeof(T), dbytes = size_t(kDFields) * n_ * sizeof(double);
+    if (cudaMalloc(&slab_, bytes) != cudaSuccess || cudaMalloc(&dslab_, dbytes) != cudaSuccess) {
       cudaGetLastError();
-      err = "device allocation of " + std::to_string(bytes) + " bytes failed";
+      err = "device allocation of " + std::to_string(bytes + dbytes) + " bytes failed";
       return QUASI_ERR_NOMEM;
     }
-    if (!cuda_ok(cudaMemset(slab_, 0, bytes), "memset")) return QUASI_ERR_CUDA;
+    if (!cuda_ok(cudaMemset(slab_, 0, bytes), "memset") || !cuda_ok(cudaMemset(dslab_, 0, dbytes), "memset"))
+      return QUASI_ERR_CUDA;
     if (!cuda_ok(cudaMalloc(&nloop_dev_, sizeof(int)), "malloc") || !cuda_ok(cudaMemset(nloop_dev_, 0, sizeof(int)), "memset"))
       return QUASI_ERR_CUDA;
     if (!cuda_ok(cudaMalloc(&partial_, (kDiagBlocks * 4 + 4) * sizeof(double)), "malloc")) return QUASI_ERR_CUDA;
@@ -110,7 +123,7 @@ class Engine : public EngineBase {
       return QUASI_ERR_CUDA;
     if (!cuda_ok(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, cfg_.device), "attribute"))
       return QUASI_ERR_CUDA;
-    if (!cuda_ok(cudaMallocHost(&host_stage_, n_ * sizeof(T) + 64), "host alloc")) return QUASI_ERR_NOMEM;
+    if (!cuda_ok(cudaMallocHost(&host_stage_, n_ * sizeof(double) + 64), "host alloc")) return QUASI_ERR_NOMEM;
     // wavenumber tables, quasi.cpp:397-431
     const int len[3] = {g_.nx, g_.ny, g_.nz};
     std::vector<double> h;
@@ -130,6 +143,15 @@ class Engine : public EngineBase {
     for (int a = 0; a < 3; ++a)
       if (!cuda_ok(tw_[a].upload(len[a]), "twiddles")) return QUASI_ERR_CUDA;
     for (int a = 0; a < 3; ++a) tb_.t[a] = tw_[a].tables();
+    if constexpr (kStateCopy<T>) {   // the double transforms' own tables
+      for (int a = 0; a < 3; ++a)
+        if (!cuda_ok(tw64_[a].upload(len[a]), "twiddles")) return QUASI_ERR_CUDA;
+      for (int a = 0; a < 3; ++a) tb64_.t[a] = tw64_[a].tables();
+    } else {
+      for (int a = 0; a < 3; ++a)
+        tb64_.t[a] = Tables<double>{reinterpret_cast<const Cx<double>*>(tb_.t[a].root),
+                                    reinterpret_cast<const Cx<double>*>(tb_.t[a].quarter)};
+    }
     build_ctx(h);
     // the six step graphs are made here, like the reference's FFTW plans
     // before its loop: quasi_step only launches them
@@ -138,11 +160,23 @@ class Engine : public EngineBase {
 
   int set_psi(const double* host) override {
     set_phase(0);   // quasi_init starts the rotation at phase 0
-    T* st = static_cast<T*>(host_stage_);
+    double* st = static_cast<double*>(host_stage_);
+    bool finite = true;
+    std::mutex mu;
     host_parallel(n_, [&](size_t lo, size_t hi) {
-      for (size_t i = lo; i < hi; ++i) st[i] = T(host[i]);
+      bool ok = true;
+      for (size_t i = lo; i < hi; ++i) {
+        st[i] = host[i];
+        ok = ok && std::isfinite(host[i]);
+      }
+      if (!ok) {
+        std::lock_guard<std::mutex> lk(mu);
+        finite = false;
+      }
     });
-    if (!cuda_ok(cudaMemcpyAsync(c_.psi, st, n_ * sizeof(T), cudaMemcpyHostToDevice, stream_), "H2D")) return QUASI_ERR_CUDA;
+    if (!finite) { err = "initial psi has a NaN or infinite value"; return QUASI_ERR_INVALID; }
+    if (!cuda_ok(cudaMemcpyAsync(c_.psi, st, n_ * sizeof(double), cudaMemcpyHostToDevice, stream_), "H2D"))
+      return QUASI_ERR_CUDA;
     if (!cuda_ok(cudaStreamSynchronize(stream_), "sync")) return QUASI_ERR_CUDA;
     have_psi_ = true;
     initialized_ = false;
@@ -153,7 +187,7 @@ class Engine : public EngineBase {
     if (!have_psi_) { err = "quasi_init before quasi_set_psi"; return QUASI_ERR_STATE; }
     set_phase(0);
     use_tma();
-    if (!cuda_ok(enqueue_init<T>(c_, tb_, nloop_dev_, stream_), "init")) return QUASI_ERR_CUDA;
+    if (!cuda_ok(enqueue_init<T>(c_, tb_, tb64_, nloop_dev_, stream_), "init")) return QUASI_ERR_CUDA;
     if (!cuda_ok(cudaStreamSynchronize(stream_), "init sync")) return QUASI_ERR_CUDA;
     nloop_ = 0;
     initialized_ = true;
@@ -185,13 +219,18 @@ class Engine : public EngineBase {
 
   int get_field(int field, double* host) override {
     set_phase(nloop_);
-    const T* src = field_ptr(field);
-    if (!src) { err = "unknown or unavailable field " + std::to_string(field); return QUASI_ERR_INVALID; }
-    T* st = static_cast<T*>(host_stage_);
-    if (!cuda_ok(cudaMemcpyAsync(st, src, n_ * sizeof(T), cudaMemcpyDeviceToHost, stream_), "D2H")) return QUASI_ERR_CUDA;
+    const Field f = field_ptr(field);
+    if (!f.p) { err = "unknown or unavailable field " + std::to_string(field); return QUASI_ERR_INVALID; }
+    if (!cuda_ok(cudaMemcpyAsync(host_stage_, f.p, n_ * f.elem, cudaMemcpyDeviceToHost, stream_), "D2H"))
+      return QUASI_ERR_CUDA;
     if (!cuda_ok(cudaStreamSynchronize(stream_), "sync")) return QUASI_ERR_CUDA;
     host_parallel(n_, [&](size_t lo, size_t hi) {
-      for (size_t i = lo; i < hi; ++i) host[i] = double(st[i]);
+      if (f.elem == sizeof(double)) {
+        std::memcpy(host + lo, static_cast<const double*>(host_stage_) + lo, (hi - lo) * sizeof(double));
+      } else {
+        const float* st = static_cast<const float*>(host_stage_);
+        for (size_t i = lo; i < hi; ++i) host[i] = double(st[i]);
+      }
     });
     return QUASI_OK;
   }
@@ -200,8 +239,8 @@ class Engine : public EngineBase {
     if (!initialized_) { err = "diagnostics before quasi_init"; return QUASI_ERR_STATE; }
     const int energy = cfg_.variant == QUASI_VARIANT_QUASI;
     set_phase(nloop_);
-    diag_partial_kernel<T><<<kDiagBlocks, kDiagThreads, 0, stream_>>>(c_.psi, c_.psi_old, c_.rho, c_.df, c_.ep, c_.alpha,
-                                                                      c_.beta, c_.gamma, energy, n_, partial_);
+    diag_partial_kernel<double, double, T><<<kDiagBlocks, kDiagThreads, 0, stream_>>>(
+        c_.psi, c_.psi_old, c_.rho, c_.df, c_.ep, c_.alpha, c_.beta, c_.gamma, energy, n_, partial_);
     diag_final_kernel<<<1, 32, 0, stream_>>>(partial_, kDiagBlocks, partial_ + kDiagBlocks * 4);
     double r[4];
     if (!cuda_ok(cudaMemcpyAsync(r, partial_ + kDiagBlocks * 4, sizeof(r), cudaMemcpyDeviceToHost, stream_), "D2H"))
@@ -219,17 +258,18 @@ class Engine : public EngineBase {
     const int i = (int)std::lround(cfg_.q_pert / vq1), k = (int)std::lround(cfg_.q0 / vq1);
     if (i < 0 || i >= g_.nx || k < 0 || k >= g_.nz) { err = "growth probe mode outside the grid"; return QUASI_ERR_INVALID; }
     const size_t id = (size_t(i) * g_.ny + 0) * g_.nz + k;
-    T a, b;
+    double a, b;
     set_phase(nloop_);
-    if (!cuda_ok(cudaMemcpyAsync(&a, c_.psiq + id, sizeof(T), cudaMemcpyDeviceToHost, stream_), "D2H") ||
-        !cuda_ok(cudaMemcpyAsync(&b, c_.psiq_old + id, sizeof(T), cudaMemcpyDeviceToHost, stream_), "D2H") ||
+    if (!cuda_ok(cudaMemcpyAsync(&a, c_.psiq + id, sizeof(double), cudaMemcpyDeviceToHost, stream_), "D2H") ||
+        !cuda_ok(cudaMemcpyAsync(&b, c_.psiq_old + id, sizeof(double), cudaMemcpyDeviceToHost, stream_), "D2H") ||
         !cuda_ok(cudaStreamSynchronize(stream_), "sync"))
       return QUASI_ERR_CUDA;
-    *out = (double(a) - double(b)) / (cfg_.dt * double(b));
+    *out = (a - b) / (cfg_.dt * b);
     return QUASI_OK;
   }
 
-  // Binary checkpoint: header + the carried state in T.
+  // Binary checkpoint: header + the carried state (each field in its own
+  // type) + a checksum of everything after the header.
   int save(const char* path) override {
     if (!initialized_) { err = "save before quasi_init"; return QUASI_ERR_STATE; }
     std::ofstream f(path, std::ios::binary);
@@ -237,10 +277,13 @@ class Engine : public EngineBase {
     Header hd = header();
     f.write(reinterpret_cast<const char*>(&hd), sizeof(hd));
     set_phase(nloop_);
-    for (T* p : carried()) {
-      if (!cuda_ok(cudaMemcpy(host_stage_, p, n_ * sizeof(T), cudaMemcpyDeviceToHost), "D2H")) return QUASI_ERR_CUDA;
-      f.write(static_cast<const char*>(host_stage_), n_ * sizeof(T));
+    uint64_t sum = kCheckSeed;
+    for (const Field& fd : carried()) {
+      if (!cuda_ok(cudaMemcpy(host_stage_, fd.p, n_ * fd.elem, cudaMemcpyDeviceToHost), "D2H")) return QUASI_ERR_CUDA;
+      sum = checksum(sum, host_stage_, n_ * fd.elem);
+      f.write(static_cast<const char*>(host_stage_), n_ * fd.elem);
     }
+    f.write(reinterpret_cast<const char*>(&sum), sizeof(sum));
     if (!f) { err = std::string("write failed: ") + path; return QUASI_ERR_IO; }
     return QUASI_OK;
   }
@@ -256,12 +299,31 @@ class Engine : public EngineBase {
       err = "checkpoint grid/variant/precision does not match the handle";
       return QUASI_ERR_IO;
     }
-    set_phase(hd.nloop);
-    for (T* p : carried()) {
-      f.read(static_cast<char*>(host_stage_), n_ * sizeof(T));
+    if (hd.nloop < 0) { err = "checkpoint step count is negative"; return QUASI_ERR_IO; }
+    // verify the whole file (length and checksum) before any of it reaches
+    // the device, so that a failed load leaves the handle as it was; then
+    // read it again field by field
+    const std::vector<Field> fields = carried_at(hd.nloop);
+    uint64_t sum = kCheckSeed;
+    for (const Field& fd : fields) {
+      f.read(static_cast<char*>(host_stage_), std::streamsize(n_ * fd.elem));
       if (!f) { err = "checkpoint is truncated"; return QUASI_ERR_IO; }
-      if (!cuda_ok(cudaMemcpy(p, host_stage_, n_ * sizeof(T), cudaMemcpyHostToDevice), "H2D")) return QUASI_ERR_CUDA;
+      sum = checksum(sum, host_stage_, n_ * fd.elem);
     }
+    uint64_t stored = 0;
+    f.read(reinterpret_cast<char*>(&stored), sizeof(stored));
+    if (!f) { err = "checkpoint is truncated"; return QUASI_ERR_IO; }
+    if (f.peek() != std::char_traits<char>::eof()) { err = "checkpoint has trailing bytes"; return QUASI_ERR_IO; }
+    if (sum != stored) { err = "checkpoint checksum mismatch (corrupt file)"; return QUASI_ERR_IO; }
+    f.clear();
+    f.seekg(sizeof(Header));
+    for (const Field& fd : fields) {
+      f.read(static_cast<char*>(host_stage_), std::streamsize(n_ * fd.elem));
+      if (!f) { err = "checkpoint read failed"; return QUASI_ERR_IO; }
+      if (!cuda_ok(cudaMemcpy(const_cast<void*>(fd.p), host_stage_, n_ * fd.elem, cudaMemcpyHostToDevice), "H2D"))
+        return QUASI_ERR_CUDA;
+    }
+    set_phase(hd.nloop);
     int nl = int(hd.nloop);
     if (!cuda_ok(cudaMemcpy(nloop_dev_, &nl, sizeof(int), cudaMemcpyHostToDevice), "H2D")) return QUASI_ERR_CUDA;
     nloop_ = hd.nloop;
@@ -310,9 +372,20 @@ class Engine : public EngineBase {
     int32_t nx, ny, nz, variant, elem, pad;
     int64_t nloop;
   };
+  // FNV-1a over 64-bit words (field sizes are multiples of 64 bytes)
+  static constexpr uint64_t kCheckSeed = 1469598103934665603ull;
+  static uint64_t checksum(uint64_t h, const void* p, size_t n) {
+    const unsigned char* b = static_cast<const unsigned char*>(p);
+    for (size_t i = 0; i + 8 <= n; i += 8) {
+      uint64_t w;
+      std::memcpy(&w, b + i, 8);
+      h = (h ^ w) * 1099511628211ull;
+    }
+    return h;
+  }
   Header header() const {
     Header h{};
-    std::memcpy(h.magic, "QUASICK1", 8);
+    std::memcpy(h.magic, "QUASICK2", 8);
     h.nx = g_.nx; h.ny = g_.ny; h.nz = g_.nz; h.variant = cfg_.variant; h.elem = int(sizeof(T));
     h.nloop = nloop_;
     return h;
@@ -335,10 +408,28 @@ class Engine : public EngineBase {
     return QUASI_OK;
   }
 
+  struct Field {
+    const void* p;
+    size_t elem;
+  };
   // the state a step reads (at the phase set by set_phase(nloop))
-  std::vector<T*> carried() {
-    return {c_.psiq, c_.psiq_old, c_.Nq_old, c_.rhoq, c_.rho_old, c_.rho, c_.vx, c_.vy, c_.vz,
-            c_.divv, c_.divvq, c_.psi, c_.psi_old, c_.p, c_.df};
+  std::vector<Field> carried() {
+    const size_t t = sizeof(T), d = sizeof(double);
+    std::vector<Field> v = {{c_.psiq, d}, {c_.psiq_old, d}, {c_.Nq_old, t}, {c_.rhoq, d},  {c_.rho_old, d},
+                            {c_.rho, d},  {c_.vx, t},       {c_.vy, t},     {c_.vz, t},    {c_.divv, t},
+                            {c_.divvq, t}, {c_.psi, d},     {c_.psi_old, d}, {c_.p, t},    {c_.df, t}};
+    if constexpr (kStateCopy<T>) {
+      v.push_back({c_.psiq_t, t});
+      v.push_back({c_.rhoq_t, t});
+    }
+    return v;
+  }
+  std::vector<Field> carried_at(long s) {
+    const long keep = nloop_;
+    set_phase(s);
+    std::vector<Field> v = carried();
+    set_phase(keep);
+    return v;
   }
 
   // Buffer rotation for a step that starts after `s` completed steps:
@@ -350,6 +441,10 @@ class Engine : public EngineBase {
     c_.psiq = psiq_buf_[s % 3];
     c_.psiq_old = psiq_buf_[(s + 2) % 3];
     c_.psiq_new = psiq_buf_[(s + 1) % 3];
+    if constexpr (!kStateCopy<T>) {   // the FP64 form reads the state itself
+      c_.psiq_t = reinterpret_cast<T*>(c_.psiq);
+      c_.rhoq_t = reinterpret_cast<T*>(c_.rhoq);
+    }
     c_.Nq = nq_buf_[s % 2];
     c_.Nq_old = nq_buf_[(s + 1) % 2];
     c_.psi = psi_buf_[s % 2];
@@ -397,33 +492,43 @@ class Engine : public EngineBase {
     c_.n0 = g_.nx / (cfg_.emulate_ranks > 0 ? cfg_.emulate_ranks : 1);
     c_.nloop = nloop_dev_;
     c_.store_dtpsi = quasi ? 0 : 1;
-    for (auto& b : psiq_buf_) b = next();
+    double* dfp = dslab_;
+    auto dnext = [&]() { double* p = dfp; dfp += n_; return p; };
+    for (auto& b : psiq_buf_) b = dnext();
+    c_.rhoq = dnext();
+    c_.rho = dnext(); c_.rho_old = dnext();
+    for (auto& b : psi_buf_) b = dnext();
+    c_.gx = dnext(); c_.gy = dnext(); c_.gz = dnext();
     for (auto& b : nq_buf_) b = next();
-    for (auto& b : psi_buf_) b = next();
+    if constexpr (kStateCopy<T>) {
+      c_.psiq_t = next();
+      c_.rhoq_t = next();
+    }
     set_phase(0);
-    c_.rhoq = next();
     c_.divvq = next(); c_.Sx = next(); c_.Sy = next(); c_.Sz = next();
-    c_.rho = next(); c_.rho_old = next();
     c_.vx = next(); c_.vy = next(); c_.vz = next(); c_.divv = next(); c_.p = next();
-    c_.df = next(); c_.lap = next(); c_.gx = next(); c_.gy = next(); c_.gz = next();
+    c_.df = next(); c_.lap = next();
     c_.rdx = next(); c_.rdy = next(); c_.rdz = next(); c_.ldx = next(); c_.ldy = next(); c_.ldz = next();
     c_.sh = next(); c_.dtpsi = next(); c_.tmp = next();
+    if constexpr (kStateCopy<T>) c_.tmp64 = dnext();
+    else c_.tmp64 = reinterpret_cast<double*>(c_.tmp);
   }
 
-  const T* field_ptr(int f) const {
+  Field field_ptr(int f) const {
+    const size_t t = sizeof(T), d = sizeof(double);
     switch (f) {
-      case QUASI_FIELD_PSI: return c_.psi;
-      case QUASI_FIELD_RHO: return c_.rho;
-      case QUASI_FIELD_VX: return c_.vx;
-      case QUASI_FIELD_VY: return c_.vy;
-      case QUASI_FIELD_VZ: return c_.vz;
-      case QUASI_FIELD_P: return c_.p;
-      case QUASI_FIELD_DIVV: return c_.divv;
-      case QUASI_FIELD_PSIQ: return c_.psiq;
-      case QUASI_FIELD_PSIQ_OLD: return c_.psiq_old;
-      case QUASI_FIELD_DTPSI: return cfg_.variant == QUASI_VARIANT_STB ? c_.dtpsi : nullptr;
-      case QUASI_FIELD_DF: return c_.df;
-      default: return nullptr;
+      case QUASI_FIELD_PSI: return {c_.psi, d};
+      case QUASI_FIELD_RHO: return {c_.rho, d};
+      case QUASI_FIELD_VX: return {c_.vx, t};
+      case QUASI_FIELD_VY: return {c_.vy, t};
+      case QUASI_FIELD_VZ: return {c_.vz, t};
+      case QUASI_FIELD_P: return {c_.p, t};
+      case QUASI_FIELD_DIVV: return {c_.divv, t};
+      case QUASI_FIELD_PSIQ: return {c_.psiq, d};
+      case QUASI_FIELD_PSIQ_OLD: return {c_.psiq_old, d};
+      case QUASI_FIELD_DTPSI: return {cfg_.variant == QUASI_VARIANT_STB ? c_.dtpsi : nullptr, t};
+      case QUASI_FIELD_DF: return {c_.df, t};
+      default: return {nullptr, t};
     }
   }
 
@@ -442,7 +547,7 @@ class Engine : public EngineBase {
     use_tma();
     if (!cuda_ok(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture"))
       return QUASI_ERR_CUDA;
-    cudaError_t e = enqueue_step<T>(c_, tb_, nloop_dev_, stream_, stream2_, fork_ev_);
+    cudaError_t e = enqueue_step<T>(c_, tb_, tb64_, nloop_dev_, stream_, stream2_, fork_ev_);
     cudaError_t e2 = cudaStreamEndCapture(stream_, &graph);
     if (!cuda_ok(e, "enqueue step") || !cuda_ok(e2, "end capture")) {
       if (graph) cudaGraphDestroy(graph);
@@ -470,6 +575,7 @@ class Engine : public EngineBase {
   cudaStream_t stream_ = nullptr;
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
   void* slab_ = nullptr;
+  double* dslab_ = nullptr;   // the double fields
   double* tabs_ = nullptr;
   int* nloop_dev_ = nullptr;
   double* partial_ = nullptr;
@@ -479,12 +585,14 @@ class Engine : public EngineBase {
   int sms_ = 148;
   void* host_stage_ = nullptr;
   DevTwiddles<T> tw_[3];
+  DevTwiddles<double> tw64_[3];   // FP32 form: the double transforms' tables
   AxisTables<T> tb_{};
+  AxisTables<double> tb64_{};
   StepCtx<T> c_{};
   cudaGraphExec_t graph_exec_[kPhases] = {};
-  T* psiq_buf_[3] = {};
+  double* psiq_buf_[3] = {};
   T* nq_buf_[2] = {};
-  T* psi_buf_[2] = {};
+  double* psi_buf_[2] = {};
   int graph_kernels_ = 0;
   long nloop_ = 0;
 };

@@ -7,7 +7,15 @@
 //
 // Templated on the storage/transform type T (double: the plain FP64 form;
 // float: the FP32 form).  Wavenumbers, spectral constants, the semi-implicit
-// update and all reductions are evaluated in double in both forms.
+// update and all reductions are evaluated in double in both forms, and both
+// keep in double what the density is built from: the carried spectral state
+// psi^, psi and grad psi (and their transforms), the density law, rho^ with
+// its Gaussian filter, rho, rho_old and the divv difference quotient.  The
+// quotient (rho - rho_old)/dt (quasi.cpp:1279) amplifies step-to-step
+// rounding noise of rho by 1/dt = 1000, and the rounding errors of a float
+// transform of psi^ lie next to psi's own spectrum (|q| = q0): the density
+// law's demodulation sqrt(q0^2 psi^2 + |grad psi|^2) moves them to the low
+// wavenumbers that the Gaussian filter keeps.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -32,13 +40,24 @@ struct StepCtx {
   // spectral state (scaled as the reference scales them).  psiq, psiq_old and
   // psiq_new rotate through three buffers and Nq, Nq_old through two (one
   // captured graph per phase of the rotation), so the update writes its
-  // result into a buffer nobody reads in that pass.
-  T *psiq, *psiq_old, *psiq_new, *Nq, *Nq_old, *rhoq, *divvq, *Sx, *Sy, *Sz;
-  // real fields (psi, psi_old and psi_new rotate through two buffers:
-  // psi_new is psi_old's buffer)
-  T *psi, *psi_old, *psi_new, *rho, *rho_old, *vx, *vy, *vz, *divv, *p, *df, *lap;
-  T *gx, *gy, *gz, *rdx, *rdy, *rdz, *ldx, *ldy, *ldz, *sh, *dtpsi, *tmp;
+  // result into a buffer nobody reads in that pass.  psiq and rhoq are held
+  // in double; in the FP32 form psiq_t and rhoq_t are their float copies,
+  // which the float transforms read (the update and the density filter write
+  // both).  In the FP64 form the copies are the fields themselves.
+  double *psiq, *psiq_old, *psiq_new, *rhoq;
+  T *psiq_t, *rhoq_t;
+  T *Nq, *Nq_old, *divvq, *Sx, *Sy, *Sz;
+  // the density and its previous value, psi and grad psi, in double (psi,
+  // psi_old and psi_new rotate through two buffers: psi_new is psi_old's
+  // buffer); tmp64: the scratch of the double transform of psi
+  double *rho, *rho_old, *psi, *psi_old, *psi_new, *gx, *gy, *gz, *tmp64;
+  // real fields in the storage type
+  T *vx, *vy, *vz, *divv, *p, *df, *lap;
+  T *rdx, *rdy, *rdz, *ldx, *ldy, *ldz, *sh, *dtpsi, *tmp;
 };
+
+// The FP32 form keeps separate float copies of psi^ and rho^.
+template <typename T> constexpr bool kStateCopy = !std::is_same<T, double>::value;
 
 __device__ __forceinline__ double sq(double x) { return x * x; }
 
@@ -131,35 +150,52 @@ template <typename T, int A, bool LAP> struct MGrad {
 };
 
 // ---------------------------------------------------------------------------
-// Real-space loaders (first, z-axis pass of forward transforms)
-// ---------------------------------------------------------------------------
-
-template <typename T> struct LdRealField {
-  StepCtx<T> c;
-  const T* src;
-  __device__ T operator()(int i, int j, int k) const { return src[at(c, i, j, k)]; }
-};
-
-// ---------------------------------------------------------------------------
 // Storers
 // ---------------------------------------------------------------------------
 
 // rhoq = scale CT(rho) exp(-1.57^2 q^2 8)                     quasi.cpp:1260-1261
-// (the Gaussian as the product of its per-axis factors, in double, with one
-// rounding to the storage type: rho's rounding noise is what the divv
-// difference quotient (rho - rho_old) / dt amplifies)
-template <typename T> struct StRhoq {
-  StepCtx<T> c;
-  __device__ T value(int i, int j, int k, T v) const {
-    return T(c.scale * double(v) * (__ldg(c.fx + i) * __ldg(c.fy + j) * __ldg(c.fz + k)));
+// The storer of the last (x) pass of the FP64 transform of rho, the Gaussian
+// as the product of its per-axis factors (host tables in double).  The FP64
+// form stages the values for the pass's TMA store.
+struct StRhoq {
+  Geom g;
+  double* rhoq;
+  double scale;
+  const double *fx, *fy, *fz;
+  __device__ double value(int i, int j, int k, double v) const {
+    return scale * v * (__ldg(fx + i) * __ldg(fy + j) * __ldg(fz + k));
   }
-  __host__ __device__ T* stage_dst() const { return c.rhoq; }
-  __device__ void operator()(int i, int j, int k, T v) const { c.rhoq[at(c, i, j, k)] = value(i, j, k, v); }
-  __device__ void pair(int i, int j, int k, T a, T b) const {
-    typename Vec2<T>::type v;
+  __host__ __device__ double* stage_dst() const { return rhoq; }
+  __device__ void operator()(int i, int j, int k, double v) const { rhoq[lin(g, i, j, k)] = value(i, j, k, v); }
+  __device__ void pair(int i, int j, int k, double a, double b) const {
+    double2 v;
     v.x = value(i, j, k, a);
     v.y = value(i, j, k + 1, b);
-    *reinterpret_cast<typename Vec2<T>::type*>(c.rhoq + at(c, i, j, k)) = v;
+    *reinterpret_cast<double2*>(rhoq + lin(g, i, j, k)) = v;
+  }
+};
+// The FP32 form's storer also writes the float copy that the grad rho
+// transforms read (no staging: two outputs).
+template <typename T>
+struct StRhoqCopy {
+  StRhoq r;
+  T* rhoq_t;
+  __device__ void operator()(int i, int j, int k, double v) const {
+    const double x = r.value(i, j, k, v);
+    const size_t id = lin(r.g, i, j, k);
+    r.rhoq[id] = x;
+    rhoq_t[id] = T(x);
+  }
+  __device__ void pair(int i, int j, int k, double a, double b) const {
+    double2 v;
+    v.x = r.value(i, j, k, a);
+    v.y = r.value(i, j, k + 1, b);
+    const size_t id = lin(r.g, i, j, k);
+    *reinterpret_cast<double2*>(r.rhoq + id) = v;
+    typename Vec2<T>::type w;
+    w.x = T(v.x);
+    w.y = T(v.y);
+    *reinterpret_cast<typename Vec2<T>::type*>(rhoq_t + id) = w;
   }
 };
 
@@ -186,50 +222,73 @@ template <typename T>
 __device__ __forceinline__ void stp(T* p, size_t pi, const Pack<T>& r) {
   reinterpret_cast<typename Vec4<T>::type*>(p)[pi] = *reinterpret_cast<const typename Vec4<T>::type*>(r.v);
 }
+// The double fields beside a pack of V = 16/sizeof(T) elements of a T field:
+// the same V elements, in 16-byte loads and stores.
+template <int V>
+struct DPack {
+  double v[V];
+};
+template <int V>
+__device__ __forceinline__ DPack<V> ldd(const double* p, size_t pi) {
+  DPack<V> r;
+#pragma unroll
+  for (int q = 0; q < V / 2; ++q)
+    *reinterpret_cast<double2*>(r.v + 2 * q) = reinterpret_cast<const double2*>(p + pi * V)[q];
+  return r;
+}
+template <int V>
+__device__ __forceinline__ void std_(double* p, size_t pi, const DPack<V>& r) {
+#pragma unroll
+  for (int q = 0; q < V / 2; ++q)
+    reinterpret_cast<double2*>(p + pi * V)[q] = *reinterpret_cast<const double2*>(r.v + 2 * q);
+}
 #define QUASI_PACKS(n)                                                                                   \
   for (size_t pi = blockIdx.x * size_t(blockDim.x) + threadIdx.x; pi < (n) / Pack<T>::V;               \
        pi += size_t(gridDim.x) * blockDim.x)
 
 // rho = kp sqrt(q0^2 psi^2 + |grad psi|^2) + rho_0   quasi.cpp:1243-1247
+// (in double, into the double scratch of the FP64 transform that follows)
 template <typename T>
 __global__ void __launch_bounds__(256) rho_law_kernel(StepCtx<T> c, size_t n) {
-  using A = Arith<T>;
   constexpr int V = Pack<T>::V;
-  const A kp = A(c.kp), q02 = A(c.q0 * c.q0), r0 = A(c.rho0);
+  const double kp = c.kp, q02 = c.q0 * c.q0, r0 = c.rho0;
   QUASI_PACKS(n) {
-    const Pack<T> ps = ldp(c.psi, pi), x = ldp(c.gx, pi), y = ldp(c.gy, pi), z = ldp(c.gz, pi);
-    Pack<T> r;
+    const DPack<V> ps = ldd<V>(c.psi, pi), x = ldd<V>(c.gx, pi), y = ldd<V>(c.gy, pi), z = ldd<V>(c.gz, pi);
+    DPack<V> r;
 #pragma unroll
     for (int u = 0; u < V; ++u) {
-      const A p = ps.v[u], a = x.v[u], b = y.v[u], d = z.v[u];
-      r.v[u] = T(kp * sqrt(q02 * p * p + a * a + b * b + d * d) + r0);
+      const double p = ps.v[u], a = x.v[u], b = y.v[u], d = z.v[u];
+      r.v[u] = kp * sqrt(q02 * p * p + a * a + b * b + d * d) + r0;
     }
-    stp(c.rho, pi, r);
+    std_(c.rho, pi, r);
   }
 }
 
 // divv (after the switch) and rho_old <- rho          quasi.cpp:1273-1289
+// The difference quotient in double from the double rho and rho_old; the
+// advection term v . grad rho from the storage-type fields.
 template <typename T>
 __global__ void __launch_bounds__(256) divv_kernel(StepCtx<T> c, size_t n) {
-  using A = Arith<T>;
   constexpr int V = Pack<T>::V;
   const bool on = *c.nloop > c.divv_switch;
-  const A idt = A(1.0 / c.dt);
+  const double idt = 1.0 / c.dt;
   QUASI_PACKS(n) {
-    const Pack<T> r = ldp(c.rho, pi);
+    const DPack<V> r = ldd<V>(c.rho, pi);
     if (on) {
-      const Pack<T> ro = ldp(c.rho_old, pi), vx = ldp(c.vx, pi), vy = ldp(c.vy, pi), vz = ldp(c.vz, pi);
+      const DPack<V> ro = ldd<V>(c.rho_old, pi);
+      const Pack<T> vx = ldp(c.vx, pi), vy = ldp(c.vy, pi), vz = ldp(c.vz, pi);
       const Pack<T> ax = ldp(c.rdx, pi), ay = ldp(c.rdy, pi), az = ldp(c.rdz, pi);
       Pack<T> dv;
 #pragma unroll
       for (int u = 0; u < V; ++u) {
-        const A rr = r.v[u], o = ro.v[u];
-        const A adv = A(vx.v[u]) * A(ax.v[u]) + A(vy.v[u]) * A(ay.v[u]) + A(vz.v[u]) * A(az.v[u]);
-        dv.v[u] = T(-((rr - o) * idt + adv) / (A(0.5) * (rr + o)));
+        const double rr = r.v[u], o = ro.v[u];
+        const double adv = double(vx.v[u]) * double(ax.v[u]) + double(vy.v[u]) * double(ay.v[u]) +
+                           double(vz.v[u]) * double(az.v[u]);
+        dv.v[u] = T(-((rr - o) * idt + adv) / (0.5 * (rr + o)));
       }
       stp(c.divv, pi, dv);
     }
-    stp(c.rho_old, pi, r);
+    std_(c.rho_old, pi, r);
   }
 }
 
@@ -240,10 +299,11 @@ __global__ void __launch_bounds__(256) stress_kernel(StepCtx<T> c, size_t n) {
   constexpr int V = Pack<T>::V;
   const A beta = A(c.beta), gamma = A(c.gamma);
   QUASI_PACKS(n) {
-    const Pack<T> gx = ldp(c.gx, pi), gy = ldp(c.gy, pi), gz = ldp(c.gz, pi);
+    const DPack<V> gx = ldd<V>(c.gx, pi), gy = ldd<V>(c.gy, pi), gz = ldd<V>(c.gz, pi);
     Pack<T> sx, sy, sz;
     if (c.variant == kQuasi) {
-      const Pack<T> rho = ldp(c.rho, pi), lap = ldp(c.lap, pi), df = ldp(c.df, pi);
+      const DPack<V> rho = ldd<V>(c.rho, pi);
+      const Pack<T> lap = ldp(c.lap, pi), df = ldp(c.df, pi);
       const Pack<T> lx = ldp(c.ldx, pi), ly = ldp(c.ldy, pi), lz = ldp(c.ldz, pi);
 #pragma unroll
       for (int u = 0; u < V; ++u) {
@@ -254,10 +314,11 @@ __global__ void __launch_bounds__(256) stress_kernel(StepCtx<T> c, size_t n) {
         sz.v[u] = T(lr * A(gz.v[u]) - rd * A(lz.v[u]));
       }
     } else {
-      const Pack<T> psi = ldp(c.psi, pi), sh = ldp(c.sh, pi);
+      const DPack<V> psi = ldd<V>(c.psi, pi);
+      const Pack<T> sh = ldp(c.sh, pi);
 #pragma unroll
       for (int u = 0; u < V; ++u) {
-        const A ps = psi.v[u];
+        const A ps = A(psi.v[u]);
         const A mu = A(sh.v[u]) - beta * ps * ps * ps + gamma * ps * ps * ps * ps * ps;
         sx.v[u] = T(mu * A(gx.v[u]));
         sy.v[u] = T(mu * A(gy.v[u]));
@@ -427,23 +488,24 @@ __global__ void __launch_bounds__(256) nonlinear_kernel(StepCtx<T> c, size_t n) 
   const bool pcoup = *c.nloop > c.divv_switch + 1;
   const A ep = A(c.ep), beta = A(c.beta), gamma = A(c.gamma), cp = A(c.kp / (c.rho_s * c.rho_s));
   QUASI_PACKS(n) {
-    const Pack<T> psi = ldp(c.psi, pi);
+    const DPack<V> psi = ldd<V>(c.psi, pi);
     const Pack<T> vx = ldp(c.vx, pi), vy = ldp(c.vy, pi), vz = ldp(c.vz, pi);
-    const Pack<T> gx = ldp(c.gx, pi), gy = ldp(c.gy, pi), gz = ldp(c.gz, pi);
+    const DPack<V> gx = ldd<V>(c.gx, pi), gy = ldd<V>(c.gy, pi), gz = ldd<V>(c.gz, pi);
     A adv[V], p3[V], p5[V];
 #pragma unroll
     for (int u = 0; u < V; ++u) {
-      const A ps = psi.v[u];
+      const A ps = A(psi.v[u]);
       p3[u] = ps * ps * ps;
       p5[u] = p3[u] * ps * ps;
       adv[u] = A(vx.v[u]) * A(gx.v[u]) + A(vy.v[u]) * A(gy.v[u]) + A(vz.v[u]) * A(gz.v[u]);
     }
     Pack<T> out;
     if (c.variant == kQuasi) {
-      const Pack<T> rho = ldp(c.rho, pi), df = ldp(c.df, pi), lap = ldp(c.lap, pi);
+      const DPack<V> rho = ldd<V>(c.rho, pi);
+      const Pack<T> df = ldp(c.df, pi), lap = ldp(c.lap, pi);
 #pragma unroll
       for (int u = 0; u < V; ++u) {
-        const A r = rho.v[u], ps = psi.v[u];
+        const A r = A(rho.v[u]), ps = A(psi.v[u]);
         out.v[u] = T(r * (ep * ps - A(df.v[u]) + beta * p3[u] - gamma * p5[u]) - r * A(lap.v[u]) - adv[u]);
       }
       if (pcoup) {
@@ -487,11 +549,12 @@ __global__ void __launch_bounds__(256) update_kernel(StepCtx<T> c) {
     const int i = row / g.ny, j = row - i * g.ny;
     const double qxy = sq(c.vqx[i]) + sq(c.vqy[j]);
     const size_t pi = size_t(row) * ppr + threadIdx.x;
-    const Pack<T> pq = ldp(c.psiq, pi), nq = ldp(c.Nq, pi);
+    const DPack<V> pq = ldd<V>(c.psiq, pi);
+    const Pack<T> nq = ldp(c.Nq, pi);
     const Pack<T> nqo = first ? nq : ldp(c.Nq_old, pi);   // :1936-1938
-    Pack<T> pqo;
-    if (c.variant == kQuasi) pqo = ldp(c.psiq_old, pi);
-    Pack<T> out;
+    DPack<V> pqo;
+    if (c.variant == kQuasi) pqo = ldd<V>(c.psiq_old, pi);
+    DPack<V> out;
 #pragma unroll
     for (int u = 0; u < V; ++u) {
       const double q2 = qxy + qz2[u];
@@ -505,9 +568,15 @@ __global__ void __launch_bounds__(256) update_kernel(StepCtx<T> c) {
         const double c1 = 1.0 + dtd2 * alin, c2 = 1.0 - dtd2 * alin;   // quasi-stb.cpp:855-856
         nv = (c1 * double(pq.v[u]) + forcing) / c2;
       }
-      out.v[u] = T(nv);
+      out.v[u] = nv;
     }
-    stp(c.psiq_new, pi, out);
+    std_(c.psiq_new, pi, out);
+    if constexpr (kStateCopy<T>) {   // the float copy the next step's transforms read
+      Pack<T> t;
+#pragma unroll
+      for (int u = 0; u < V; ++u) t.v[u] = T(out.v[u]);
+      stp(c.psiq_t, pi, t);
+    }
   }
 }
 
@@ -630,9 +699,11 @@ inline dim3 row_block(int nz) {
 // density chain after the gradients), so that in
 // the captured graph one persistent pass kernel's last tiles overlap the next
 // one's first loads.  s2 == nullptr: everything on s.
+// tb64: the FP64 twiddles of the double transforms (the same tables as tb in
+// the FP64 form).
 template <typename T>
-cudaError_t enqueue_step(const StepCtx<T>& c, const AxisTables<T>& tb, int* nloop_dev, cudaStream_t s,
-                         cudaStream_t s2 = nullptr, const cudaEvent_t* ev = nullptr) {
+cudaError_t enqueue_step(const StepCtx<T>& c, const AxisTables<T>& tb, const AxisTables<double>& tb64, int* nloop_dev,
+                         cudaStream_t s, cudaStream_t s2 = nullptr, const cudaEvent_t* ev = nullptr) {
   const Geom g = c.g;
   const size_t n = size_t(g.nx) * g.ny * g.nz;
   const cudaStream_t sb = s2 ? s2 : s;
@@ -650,17 +721,32 @@ cudaError_t enqueue_step(const StepCtx<T>& c, const AxisTables<T>& tb, int* nloo
   QUASI_TRY(cudaGetLastError());
   auto st = [&](T* d) { return StoreField<T>{g, d}; };
   auto ld = [&](T* d) { return LoadField<T>{g, d}; };
+  auto st64 = [&](double* d) { return StoreField<double>{g, d}; };
   if (c.variant == kQuasi) {
     // a3 prologue quasi.cpp:1036-1057
     // (pairs that share the source, kinds and shift take one dual x pass)
     // a4 gradients quasi.cpp:1120-1232: grad psi with grad lap grad psi, grad rho
     QUASI_TRY(fork(0));
-    QUASI_TRY(inverse3_mul2(g, tb, kiSTx, c.psiq, MGrad<T, 0, false>{c}, MGrad<T, 0, true>{c}, 1, 0, 0, c.gx, c.ldx, s));
-    QUASI_TRY(inverse3_mul2(g, tb, kiSTy, c.psiq, MGrad<T, 1, false>{c}, MGrad<T, 1, true>{c}, 0, 1, 0, c.gy, c.ldy, sb));
-    QUASI_TRY(inverse3_mul2(g, tb, kiSTz, c.psiq, MGrad<T, 2, false>{c}, MGrad<T, 2, true>{c}, 0, 0, 1, c.gz, c.ldz, s));
-    QUASI_TRY(inverse3_mul(g, tb, kiSTx, c.rhoq, MGrad<T, 0, false>{c}, 1, 0, 0, st(c.rdx), c.rdx, sb));
-    QUASI_TRY(inverse3_mul(g, tb, kiSTy, c.rhoq, MGrad<T, 1, false>{c}, 0, 1, 0, st(c.rdy), c.rdy, s));
-    QUASI_TRY(inverse3_mul(g, tb, kiSTz, c.rhoq, MGrad<T, 2, false>{c}, 0, 0, 1, st(c.rdz), c.rdz, sb));
+    if constexpr (kStateCopy<T>) {
+      // grad psi in double from psi^ itself; grad lap grad psi in float from its copy
+      QUASI_TRY(inverse3_mul(g, tb64, kiSTx, c.psiq, MGrad<T, 0, false>{c}, 1, 0, 0, st64(c.gx), c.gx, s));
+      QUASI_TRY(inverse3_mul(g, tb, kiSTx, c.psiq_t, MGrad<T, 0, true>{c}, 1, 0, 0, st(c.ldx), c.ldx, sb));
+      QUASI_TRY(inverse3_mul(g, tb64, kiSTy, c.psiq, MGrad<T, 1, false>{c}, 0, 1, 0, st64(c.gy), c.gy, sb));
+      QUASI_TRY(inverse3_mul(g, tb, kiSTy, c.psiq_t, MGrad<T, 1, true>{c}, 0, 1, 0, st(c.ldy), c.ldy, s));
+      QUASI_TRY(inverse3_mul(g, tb64, kiSTz, c.psiq, MGrad<T, 2, false>{c}, 0, 0, 1, st64(c.gz), c.gz, s));
+      QUASI_TRY(inverse3_mul(g, tb, kiSTz, c.psiq_t, MGrad<T, 2, true>{c}, 0, 0, 1, st(c.ldz), c.ldz, sb));
+    } else {
+      // one dual x pass per axis: grad psi with grad lap grad psi
+      QUASI_TRY(inverse3_mul2(g, tb, kiSTx, c.psiq_t, MGrad<T, 0, false>{c}, MGrad<T, 0, true>{c}, 1, 0, 0,
+                              reinterpret_cast<T*>(c.gx), c.ldx, s));
+      QUASI_TRY(inverse3_mul2(g, tb, kiSTy, c.psiq_t, MGrad<T, 1, false>{c}, MGrad<T, 1, true>{c}, 0, 1, 0,
+                              reinterpret_cast<T*>(c.gy), c.ldy, sb));
+      QUASI_TRY(inverse3_mul2(g, tb, kiSTz, c.psiq_t, MGrad<T, 2, false>{c}, MGrad<T, 2, true>{c}, 0, 0, 1,
+                              reinterpret_cast<T*>(c.gz), c.ldz, s));
+    }
+    QUASI_TRY(inverse3_mul(g, tb, kiSTx, c.rhoq_t, MGrad<T, 0, false>{c}, 1, 0, 0, st(c.rdx), c.rdx, sb));
+    QUASI_TRY(inverse3_mul(g, tb, kiSTy, c.rhoq_t, MGrad<T, 1, false>{c}, 0, 1, 0, st(c.rdy), c.rdy, s));
+    QUASI_TRY(inverse3_mul(g, tb, kiSTz, c.rhoq_t, MGrad<T, 2, false>{c}, 0, 0, 1, st(c.rdz), c.rdz, sb));
     // the density chain needs grad psi and must not rewrite rho^ before the grad
     // rho transforms have read it: s waits for the second stream's share ...
     if (s2) {
@@ -668,21 +754,26 @@ cudaError_t enqueue_step(const StepCtx<T>& c, const AxisTables<T>& tb, int* nloo
       QUASI_TRY(cudaStreamWaitEvent(s, ev[7], 0));
     }
     // ... which then runs a3's prologue quasi.cpp:1036-1057 beside it
-    QUASI_TRY(inverse3_mul2(g, tb, kiCT, c.psiq, MDf<T>{c}, MLap<T>{c}, 0, 0, 0, c.df, c.lap, sb));
-    // a5 density + filter quasi.cpp:1237-1268 (rho doubles as the scratch)
+    QUASI_TRY(inverse3_mul2(g, tb, kiCT, c.psiq_t, MDf<T>{c}, MLap<T>{c}, 0, 0, 0, c.df, c.lap, sb));
+    // a5 density + filter quasi.cpp:1237-1268 in double (rho doubles as the
+    // scratch of its transform)
     QUASI_EW(rho_law_kernel<T>, c, n);
     QUASI_TRY(cudaGetLastError());
-    QUASI_TRY(forward3(g, tb, kCT, ld(c.rho), c.rho, StRhoq<T>{c}, s));
-    QUASI_TRY(inverse3(g, tb, kiCT, ld(c.rhoq), c.rho, st(c.rho), s));
+    const StRhoq sr{g, c.rhoq, c.scale, c.fx, c.fy, c.fz};
+    if constexpr (kStateCopy<T>)
+      QUASI_TRY(forward3(g, tb64, kCT, LoadField<double>{g, c.rho}, c.rho, StRhoqCopy<T>{sr, c.rhoq_t}, s));
+    else
+      QUASI_TRY(forward3(g, tb64, kCT, LoadField<double>{g, c.rho}, c.rho, sr, s));
+    QUASI_TRY(inverse3(g, tb64, kiCT, LoadField<double>{g, c.rhoq}, c.rho, st64(c.rho), s));
     QUASI_TRY(join(0));
 
   } else {
     // quasi-stb.cpp:1005-1038 (the unused dRho transform is elided)
     QUASI_TRY(fork(0));
-    QUASI_TRY(inverse3_mul(g, tb, kiCT, c.psiq, MSh<T>{c}, 0, 0, 0, st(c.sh), c.sh, s));
-    QUASI_TRY(inverse3_mul(g, tb, kiSTx, c.psiq, MGrad<T, 0, false>{c}, 1, 0, 0, st(c.gx), c.gx, sb));
-    QUASI_TRY(inverse3_mul(g, tb, kiSTy, c.psiq, MGrad<T, 1, false>{c}, 0, 1, 0, st(c.gy), c.gy, s));
-    QUASI_TRY(inverse3_mul(g, tb, kiSTz, c.psiq, MGrad<T, 2, false>{c}, 0, 0, 1, st(c.gz), c.gz, sb));
+    QUASI_TRY(inverse3_mul(g, tb, kiCT, c.psiq_t, MSh<T>{c}, 0, 0, 0, st(c.sh), c.sh, s));
+    QUASI_TRY(inverse3_mul(g, tb64, kiSTx, c.psiq, MGrad<T, 0, false>{c}, 1, 0, 0, st64(c.gx), c.gx, sb));
+    QUASI_TRY(inverse3_mul(g, tb64, kiSTy, c.psiq, MGrad<T, 1, false>{c}, 0, 1, 0, st64(c.gy), c.gy, s));
+    QUASI_TRY(inverse3_mul(g, tb64, kiSTz, c.psiq, MGrad<T, 2, false>{c}, 0, 0, 1, st64(c.gz), c.gz, sb));
     QUASI_TRY(join(0));
     // rho == 1, divv == 0, grad rho == 0 (rhoq never leaves 0): quasi-stb.cpp:1232
   }
@@ -736,7 +827,8 @@ cudaError_t enqueue_step(const StepCtx<T>& c, const AxisTables<T>& tb, int* nloo
     update_kernel<T><<<per_sm * tma_config().sms, blk, 0, s>>>(c);
   }
   QUASI_TRY(cudaGetLastError());
-  QUASI_TRY(inverse3(g, tb, kiCT, ld(c.psiq_new), c.tmp, st(c.psi_new), s));   // psi_old <- psi by rotation
+  // psi = iCT(psiq_new) in double; psi_old <- psi by rotation
+  QUASI_TRY(inverse3(g, tb64, kiCT, LoadField<double>{g, c.psiq_new}, c.tmp64, st64(c.psi_new), s));
   return cudaSuccess;
 }
 
@@ -759,23 +851,38 @@ __global__ void init_state_kernel(StepCtx<T> c, size_t n) {
     c.psi_old[id] = c.psi[id];   // quasi.cpp:948
     c.divv[id] = T(0);
     c.divvq[id] = T(0);
-    c.rhoq[id] = T(0);
-    c.rho_old[id] = T(0);
+    c.rhoq[id] = 0.0;
+    if constexpr (kStateCopy<T>) c.rhoq_t[id] = T(0);
+    c.rho_old[id] = 0.0;
     c.vx[id] = T(0);
     c.vy[id] = T(0);
     c.vz[id] = T(0);
     c.p[id] = T(0);
-    c.rho[id] = c.variant == kQuasi ? T(0) : T(1);
+    c.rho[id] = c.variant == kQuasi ? 0.0 : 1.0;
   }
 }
 
+// double field -> storage type (the FP32 form's copy of psi^ after the pre-loop)
 template <typename T>
-cudaError_t enqueue_init(const StepCtx<T>& c, const AxisTables<T>& tb, int* nloop_dev, cudaStream_t s) {
+__global__ void to_storage_kernel(const double* src, T* dst, size_t n) {
+  for (size_t id = blockIdx.x * size_t(blockDim.x) + threadIdx.x; id < n; id += size_t(gridDim.x) * blockDim.x)
+    dst[id] = T(src[id]);
+}
+
+// The projection psiq = scale CT(psi), psi = iCT(psiq) runs in double in both
+// forms (quasi_set_psi leaves the initial psi in c.psi).
+template <typename T>
+cudaError_t enqueue_init(const StepCtx<T>& c, const AxisTables<T>& tb, const AxisTables<double>& tb64, int* nloop_dev,
+                         cudaStream_t s) {
   const Geom g = c.g;
-  QUASI_TRY(forward3(g, tb, kCT, LdRealField<T>{c, c.psi}, c.psiq, ScaleStore<T>{g, c.psiq, T(c.scale)}, s));
-  QUASI_TRY(inverse3(g, tb, kiCT, LdRealField<T>{c, c.psiq}, c.psi, StoreField<T>{g, c.psi}, s));
-  QUASI_TRY(forward3(g, tb, kCT, LdInitN<T>{c}, c.Nq_old, StoreField<T>{g, c.Nq_old}, s));
   const size_t n = size_t(g.nx) * g.ny * g.nz;
+  QUASI_TRY(forward3(g, tb64, kCT, LoadField<double>{g, c.psi}, c.psiq, ScaleStore<double>{g, c.psiq, c.scale}, s));
+  if constexpr (kStateCopy<T>) {
+    to_storage_kernel<T><<<592, 256, 0, s>>>(c.psiq, c.psiq_t, n);
+    QUASI_TRY(cudaGetLastError());
+  }
+  QUASI_TRY(inverse3(g, tb64, kiCT, LoadField<double>{g, c.psiq}, c.psi, StoreField<double>{g, c.psi}, s));
+  QUASI_TRY(forward3(g, tb, kCT, LdInitN<T>{c}, c.Nq_old, StoreField<T>{g, c.Nq_old}, s));
   init_state_kernel<T><<<592, 256, 0, s>>>(c, n);
   QUASI_TRY(cudaGetLastError());
   QUASI_TRY(cudaMemsetAsync(nloop_dev, 0, sizeof(int), s));
