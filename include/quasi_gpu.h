@@ -38,7 +38,9 @@ enum quasi_status {
   QUASI_ERR_STATE = -4,      /* call out of order (e.g. step before init) */
   QUASI_ERR_IO = -5,         /* checkpoint file missing, short or corrupt */
   QUASI_ERR_NODEVICE = -6,   /* no usable CUDA device */
-  QUASI_ERR_UNSUPPORTED = -7 /* valid request this build does not implement */
+  QUASI_ERR_UNSUPPORTED = -7,/* valid request this build does not implement */
+  QUASI_ERR_TIMEOUT = -8     /* a kernel's bounded wait gave up (a tile copy
+                                never completed); the context stays usable */
 };
 
 enum quasi_variant {
@@ -235,6 +237,15 @@ QUASI_API int quasi_r2r_execute_device(quasi_r2r_plan* p, void* data, void* stre
 /* host doubles in -> host doubles out (may alias); copies included. */
 QUASI_API int quasi_r2r_execute_host(quasi_r2r_plan* p, const double* in, double* out);
 QUASI_API int quasi_r2r_plan_destroy(quasi_r2r_plan* p);
+
+/* Fault injection for failure-detection tests (no reference counterpart: the
+ * reference has no failure detection).  The plan's next execution issues no
+ * copy for tile `skip_tile` of each of its TMA passes and gives every tile
+ * wait `poll_limit` polls: the wait of that tile runs out, the kernel drains
+ * its other copies, flags the error and returns, and the synchronising
+ * execution returns QUASI_ERR_TIMEOUT (the output is then undefined).  Only
+ * the next execution is affected. */
+QUASI_API int quasi_r2r_inject_wait_timeout(quasi_r2r_plan* p, int skip_tile, unsigned poll_limit);
 
 #ifdef __cplusplus
 }

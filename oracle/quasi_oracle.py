@@ -144,9 +144,9 @@ def _r2r(a: np.ndarray, kinds: tuple[str, str, str]) -> np.ndarray:
     for axis, kind in enumerate(kinds):
         typ = 2 if kind.endswith("10") else 3
         if kind.startswith("E"):
-            out = sfft.dct(out, type=typ, axis=axis, norm=None)
+            out = sfft.dct(out, type=typ, axis=axis, norm=None, workers=-1)
         else:
-            out = sfft.dst(out, type=typ, axis=axis, norm=None)
+            out = sfft.dst(out, type=typ, axis=axis, norm=None, workers=-1)
     return out
 
 

@@ -213,7 +213,11 @@ class Engine : public EngineBase {
     if (!cuda_ok(cudaStreamSynchronize(stream_), "step sync")) return QUASI_ERR_CUDA;
     int tma_failed = 0;
     if (!cuda_ok(cudaMemcpy(&tma_failed, tma_err_, sizeof(int), cudaMemcpyDeviceToHost), "flag")) return QUASI_ERR_CUDA;
-    if (tma_failed) { err = "a tile copy did not complete within its wait limit"; return QUASI_ERR_CUDA; }
+    if (tma_failed) {
+      cudaMemset(tma_err_, 0, sizeof(int));
+      err = "a tile copy did not complete within its wait limit";
+      return QUASI_ERR_TIMEOUT;
+    }
     return QUASI_OK;
   }
 

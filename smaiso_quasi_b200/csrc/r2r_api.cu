@@ -17,11 +17,28 @@ struct R2RBase {
   cudaStream_t own = nullptr;
   int* tma_err = nullptr;
   int sms = 148;
+  int inject_skip = -1;             // fault injection for the next execution
+  uint32_t inject_polls = kTmaPollLimit;
   void use_tma() {
     TmaConfig& t = tma_config();
     t.err = tma_err;
     t.sms = sms;
     t.enabled = true;
+    t.skip_tile = inject_skip;
+    t.poll_limit = inject_polls;
+  }
+  void end_tma() {   // the injection lasts one execution
+    TmaConfig& t = tma_config();
+    t.skip_tile = inject_skip = -1;
+    t.poll_limit = inject_polls = kTmaPollLimit;
+  }
+  // after a synchronised execution: did a tile wait give up?
+  cudaError_t timed_out(bool* out) {
+    int f = 0;
+    cudaError_t e = cudaMemcpy(&f, tma_err, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && f) e = cudaMemset(tma_err, 0, sizeof(int));
+    *out = f != 0;
+    return e;
   }
 };
 
@@ -54,8 +71,10 @@ struct R2R : R2RBase {
     cudaError_t e;
     use_tma();
     const int k3[3] = {kind[0], kind[1], kind[2]};
-    if ((e = yz3(g, tb, k3, d, StoreField<T>{g, d}, s)) != cudaSuccess) return e;
-    return launch_pass<T, 0>(g, kind[0], tb.t[0], LoadField<T>{g, d}, StoreField<T>{g, d}, s);
+    e = yz3(g, tb, k3, d, StoreField<T>{g, d}, s);
+    if (e == cudaSuccess) e = launch_pass<T, 0>(g, kind[0], tb.t[0], LoadField<T>{g, d}, StoreField<T>{g, d}, s);
+    end_tma();
+    return e;
   }
 };
 
@@ -123,7 +142,10 @@ int quasi_r2r_execute_device(quasi_r2r_plan* p, void* data, void* stream) {
   cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : p->impl->own;
   cudaError_t e = p->impl->exec(data, s);
   if (e == cudaSuccess && !stream) e = cudaStreamSynchronize(s);
+  bool late = false;
+  if (e == cudaSuccess && !stream) e = p->impl->timed_out(&late);
   if (e != cudaSuccess) return set_error(QUASI_ERR_CUDA, cudaGetErrorString(e));
+  if (late) return set_error(QUASI_ERR_TIMEOUT, "a tile copy did not complete within its wait limit");
   return QUASI_OK;
 }
 
@@ -148,11 +170,21 @@ int quasi_r2r_execute_host(quasi_r2r_plan* p, const double* in, double* out) {
     else e = cudaMemcpyAsync(f.data(), d, n * 4, cudaMemcpyDeviceToHost, b->own);
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(b->own);
+  bool late = false;
+  if (e == cudaSuccess) e = b->timed_out(&late);
   quasi::MapCache::get().forget(d, static_cast<char*>(d) + n * b->elem);
   cudaFree(d);
   if (e != cudaSuccess) return set_error(QUASI_ERR_CUDA, cudaGetErrorString(e));
+  if (late) return set_error(QUASI_ERR_TIMEOUT, "a tile copy did not complete within its wait limit");
   if (b->elem == 4)
     for (size_t i = 0; i < n; ++i) out[i] = f[i];
+  return QUASI_OK;
+}
+
+int quasi_r2r_inject_wait_timeout(quasi_r2r_plan* p, int skip_tile, unsigned poll_limit) {
+  if (!p || skip_tile < 0 || poll_limit < 1) return set_error(QUASI_ERR_INVALID, "need a plan, skip_tile >= 0, poll_limit >= 1");
+  p->impl->inject_skip = skip_tile;
+  p->impl->inject_polls = poll_limit;
   return QUASI_OK;
 }
 

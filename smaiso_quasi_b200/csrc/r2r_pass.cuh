@@ -341,6 +341,16 @@ struct MulSrc {
 
 constexpr uint32_t kTmaPollLimit = 1u << 24;
 
+// After a timed-out wait on buffer b for tile t: the other buffer holds the
+// copy of tile t + stride unless that tile is past the end or was skipped by
+// the fault-injection hook; wait for it (bounded) so that no copy into this
+// CTA's shared memory is in flight when the CTA exits.
+__device__ __forceinline__ void drain_other(uint64_t* bar, int b, int it, int t, int stride, int ntiles, int skip,
+                                            uint32_t polls) {
+  const int t_other = t + stride;
+  if (t_other < ntiles && t_other != skip) mbar_wait_bounded(&bar[b ^ 1], ((it + 1) >> 1) & 1, polls);
+}
+
 template <int AXIS, int P>
 __device__ __forceinline__ void tile_origin(const Geom& g, int tile, int& c0, int& c1, int& c2) {
   if (AXIS == 2) {   // P rows (i, j0..j0+P-1); P divides ny
@@ -389,7 +399,7 @@ template <typename T, int N, int P> constexpr int tma_work_elems() { return ((P 
 template <typename T, int N, int AXIS, int P, class Store, class Mul, class Mul2 = NoMul, bool TSTORE = false>
 __global__ void __launch_bounds__(tma_threads<T>(), 2)
     tma_pass_kernel(const __grid_constant__ CUtensorMap map, Geom g, int kind, Tables<T> tb, Store st, int ntiles,
-                    int* err, Mul mul, int dc1, int dc2, int ks, Store st2, Mul2 mul2,
+                    int* err, uint32_t polls, int skip, Mul mul, int dc1, int dc2, int ks, Store st2, Mul2 mul2,
                     const __grid_constant__ CUtensorMap dmap, const __grid_constant__ CUtensorMap dmap2) {
   static_assert(!TSTORE || AXIS != 2, "TMA-stored tiles are x / y passes");
   constexpr bool kDual = !std::is_same<Mul2, NoMul>::value;
@@ -423,9 +433,11 @@ __global__ void __launch_bounds__(tma_threads<T>(), 2)
   __syncthreads();
   const int t0 = blockIdx.x;
   if (tid == 0) {
-    if (t0 < ntiles) tma_issue_tile<T, N, AXIS, P>(&map, raw0, &bar[0], g, t0, dc1, dc2);
+    // skip: the tile whose copy the fault-injection hook never issues (its
+    // wait then runs out); -1 outside the failure-detection tests
+    if (t0 < ntiles && t0 != skip) tma_issue_tile<T, N, AXIS, P>(&map, raw0, &bar[0], g, t0, dc1, dc2);
     if (t0 + int(gridDim.x) < ntiles)
-      tma_issue_tile<T, N, AXIS, P>(&map, raw1, &bar[1], g, t0 + gridDim.x, dc1, dc2);
+      if (t0 + int(gridDim.x) != skip) tma_issue_tile<T, N, AXIS, P>(&map, raw1, &bar[1], g, t0 + gridDim.x, dc1, dc2);
   }
   DevExec ex;
   int it = 0;
@@ -434,12 +446,13 @@ __global__ void __launch_bounds__(tma_threads<T>(), 2)
     T* raw = b ? raw1 : raw0;
     const uint32_t parity = (it >> 1) & 1;
     // every thread polls; the CTA leaves together if any poll gave up
-    const bool arrived = mbar_wait_bounded(&bar[b], parity, kTmaPollLimit);
+    const bool arrived = mbar_wait_bounded(&bar[b], parity, polls);
     if constexpr (TSTORE) {
       if (tid == 0) bulk_wait_read0();   // the previous tile's store has read the work tile
     }
     if (!__syncthreads_and(arrived)) {
       if (tid == 0) atomicExch(err, 1);
+      drain_other(bar, b, it, t, int(gridDim.x), ntiles, skip, polls);
       break;
     }
     const int t_next = t + 2 * int(gridDim.x);
@@ -461,7 +474,7 @@ __global__ void __launch_bounds__(tma_threads<T>(), 2)
       }
     };
     auto issue_next = [&]() {
-      if (tid == 0 && t_next < ntiles) {
+      if (tid == 0 && t_next < ntiles && t_next != skip) {
         fence_proxy_async_smem();
         tma_issue_tile<T, N, AXIS, P>(&map, raw, &bar[b], g, t_next, dc1, dc2);
       }
@@ -592,6 +605,8 @@ cudaError_t launch_pass_n(const Geom& g, int kind, Tables<T> tb, Load ld, Store 
 // (z: P divides ny and nz <= 256); `tma_err` receives wait timeouts.
 struct TmaConfig {
   int* err = nullptr;     // device flag, nonzero after a timed-out wait
+  uint32_t poll_limit = kTmaPollLimit;   // polls before a tile wait gives up
+  int skip_tile = -1;     // fault injection: a tile whose copy is never issued
   int sms = 148;          // CTAs per SM x SMs bounds the persistent grid
   bool enabled = true;
 };
@@ -642,8 +657,8 @@ cudaError_t launch_tma_pass(const Geom& g, int kind, Tables<T> tb, const T* src,
   else if (AXIS == 1) tiles = g.nx * (g.nz / P);
   else tiles = g.ny * (g.nz / P);
   const int grid = tiles < per_sm * tma_config().sms ? tiles : per_sm * tma_config().sms;
-  kern<<<grid, tma_threads<T>(), smem, s>>>(map, g, kind, tb, st, tiles, tma_config().err, mul, dc1, dc2, ks, st2,
-                                             mul2, dmap, dmap2);
+  kern<<<grid, tma_threads<T>(), smem, s>>>(map, g, kind, tb, st, tiles, tma_config().err, tma_config().poll_limit,
+                                             tma_config().skip_tile, mul, dc1, dc2, ks, st2, mul2, dmap, dmap2);
   return cudaGetLastError();
 }
 

@@ -337,7 +337,7 @@ template <typename T> constexpr bool zpass_root_copy() { return sizeof(T) == 4; 
 template <typename T, int N, int P, int KS>
 __global__ void __launch_bounds__(256, 2)
     tma_zpass_kernel(const __grid_constant__ CUtensorMap src_map, const __grid_constant__ CUtensorMap dst_map, Geom g,
-                     int kind, Tables<T> tb, int ntiles, int* err) {
+                     int kind, Tables<T> tb, int ntiles, int* err, uint32_t polls, int skip) {
   constexpr int NT = 256, G = P / 2, SUB = (N + 255) / 256, BN = N / SUB;
   using Z = ZTile<T, N, G, NT, SUB>;
   constexpr bool kRootCopy = zpass_root_copy<T>();
@@ -384,17 +384,18 @@ __global__ void __launch_bounds__(256, 2)
   __syncthreads();
   const int t0 = blockIdx.x;
   if (tid == 0) {
-    if (t0 < ntiles) issue(raw0, &bar[0], t0);
-    if (t0 + int(gridDim.x) < ntiles) issue(raw1, &bar[1], t0 + gridDim.x);
+    if (t0 < ntiles && t0 != skip) issue(raw0, &bar[0], t0);
+    if (t0 + int(gridDim.x) < ntiles && t0 + int(gridDim.x) != skip) issue(raw1, &bar[1], t0 + gridDim.x);
   }
   DevExec ex;
   int it = 0;
   for (int t = t0; t < ntiles; t += gridDim.x, ++it) {
     const int b = it & 1;
     T* raw = b ? raw1 : raw0;
-    const bool arrived = mbar_wait_bounded(&bar[b], (it >> 1) & 1, kTmaPollLimit);
+    const bool arrived = mbar_wait_bounded(&bar[b], (it >> 1) & 1, polls);
     if (!__syncthreads_and(arrived)) {
       if (tid == 0) atomicExch(err, 1);
+      drain_other(bar, b, it, t, int(gridDim.x), ntiles, skip, polls);
       break;
     }
     // first stage: dense rows -> registers | previous store read out | -> padded tile
@@ -402,7 +403,7 @@ __global__ void __launch_bounds__(256, 2)
     Z::first_read(tid, typename Z::template RowsK<KS>{raw}, kind, tb, r1, tw1);
     if (tid == 0) bulk_wait_read0();
     __syncthreads();
-    if (tid == 0 && t + 2 * int(gridDim.x) < ntiles) {
+    if (tid == 0 && t + 2 * int(gridDim.x) < ntiles && t + 2 * int(gridDim.x) != skip) {
       fence_proxy_async_smem();
       issue(raw, &bar[b], t + 2 * gridDim.x);
     }
@@ -451,7 +452,8 @@ cudaError_t launch_zpass_nk(const Geom& g, int kind, Tables<T> tb, const T* src,
   }
   const int tiles = (g.nx * g.ny) / P;
   const int grid = tiles < per_sm * tma_config().sms ? tiles : per_sm * tma_config().sms;
-  kern<<<grid, 256, smem, s>>>(smap, dmap, g, kind, tb, tiles, tma_config().err);
+  kern<<<grid, 256, smem, s>>>(smap, dmap, g, kind, tb, tiles, tma_config().err, tma_config().poll_limit,
+                               tma_config().skip_tile);
   return cudaGetLastError();
 }
 

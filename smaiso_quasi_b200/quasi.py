@@ -36,7 +36,7 @@ EXPORTS = [
     "quasi_diagnostics", "quasi_growth_rate", "quasi_save", "quasi_load", "quasi_r2r_plan_create",
     "quasi_r2r_execute_device", "quasi_r2r_execute_host", "quasi_r2r_plan_destroy",
     "quasi_ic_default", "quasi_initial_condition", "quasi_step_kernels", "quasi_time_axis_pass",
-    "quasi_step_async", "quasi_synchronize", "quasi_diagnostics_noalloc",
+    "quasi_step_async", "quasi_synchronize", "quasi_diagnostics_noalloc", "quasi_r2r_inject_wait_timeout",
     "quasi_ensemble_create", "quasi_ensemble_size", "quasi_ensemble_member", "quasi_ensemble_init",
     "quasi_ensemble_step", "quasi_ensemble_growth_rates", "quasi_ensemble_destroy",
 ]
@@ -105,6 +105,7 @@ def lib() -> ctypes.CDLL:
         L.quasi_r2r_execute_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         L.quasi_r2r_execute_host.argtypes = [ctypes.c_void_p, dp, dp]
         L.quasi_r2r_plan_destroy.argtypes = [ctypes.c_void_p]
+        L.quasi_r2r_inject_wait_timeout.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_uint]
         L.quasi_step_kernels.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
         L.quasi_time_axis_pass.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, dp]
         L.quasi_ic_default.argtypes = [ctypes.POINTER(IC), ctypes.c_int]
@@ -317,6 +318,11 @@ class R2RPlan:
     def execute_device(self, data_ptr: int, stream: int | None = None) -> None:
         _check(lib().quasi_r2r_execute_device(self._p, ctypes.c_void_p(data_ptr),
                                               ctypes.c_void_p(stream) if stream else None))
+
+    def inject_wait_timeout(self, skip_tile: int = 0, poll_limit: int = 64) -> None:
+        """Failure-detection test hook: the next execution skips one tile's
+        copy and raises QuasiError(QUASI_ERR_TIMEOUT)."""
+        _check(lib().quasi_r2r_inject_wait_timeout(self._p, int(skip_tile), int(poll_limit)))
 
     def close(self) -> None:
         if getattr(self, "_p", None):

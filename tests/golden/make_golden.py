@@ -37,7 +37,15 @@ CASES = [
     ("quasi_8x16x16_np4_s205", "quasi", (8, 16, 16), 4, 205, 5, 41, "undulated", 5),
     ("stb_16x16x32_np2_s6", "stb", (16, 16, 32), 2, 6, 1, 1, "stb", 3),
     ("quasi_16x16x16_np2_fc_s2", "quasi", (16, 16, 16), 2, 2, 1, 2, "focal_conic", 0),
+    # the 64x64x128 planar interface as `mpirun -np 4` runs it: 500 steps,
+    # diagnostics every 50 steps, a dump every 2nd diagnostic (kept small:
+    # psi mid-slices per dump, every field's mid-slice of the last dump, no
+    # full fields)
+    ("quasi_64x64x128_np4_s500", "quasi", (64, 64, 128), 4, 500, 50, 2, "planar", 1234),
 ]
+# cases stored without full fields (their initial psi is the seeded IC, which
+# tests regenerate)
+SLIM = {"quasi_64x64x128_np4_s500"}
 
 
 def make(case) -> None:
@@ -51,13 +59,15 @@ def make(case) -> None:
         ref = rr.run_reference(variant, nx, ny, nz, psi0, ranks, steps, l1, save, d, fc_size="6")
     nsl = nx * nz
     arrays = {}
-    if "psi" in ref:                     # quasi-stb.cpp:2051-2062 (full psi dump) is commented out
+    slim = name in SLIM
+    if "psi" in ref and not slim:        # quasi-stb.cpp:2051-2062 (full psi dump) is commented out
         arrays["psi"] = ref["psi"]
-    if psi0 is not None:
+    if psi0 is not None and not slim:
         arrays["ic"] = psi0
     slices = ["psiMid", "vx", "vy", "vz", "divv", "p", "rho"] if variant == "quasi" else ["psiMid", "dtpsi", "fourier"]
     for nm in slices:
-        arrays[nm] = ref[nm].reshape(-1, nsl)
+        a = ref[nm].reshape(-1, nsl)
+        arrays[nm] = a if (nm == "psiMid" or not slim) else a[-1:]
     for nm in ["L1", "mass", "energy", "growth"]:
         if ref[nm].size:
             arrays[nm] = ref[nm]
@@ -70,5 +80,7 @@ def make(case) -> None:
 if __name__ == "__main__":
     if not rr.available("quasi") or not rr.available("stb"):
         sys.exit("build the reference first: oracle/build_ref.sh")
+    only = set(sys.argv[1:])
     for c in CASES:
-        make(c)
+        if not only or c[0] in only:
+            make(c)

@@ -99,3 +99,34 @@ def test_c_ensemble_members_equal_lone_instances():
             s.init()
             s.step(9)
             np.testing.assert_array_equal(s.field("psi"), t)
+
+
+CONFIG1 = "quasi_64x64x128_np4_s500"
+
+
+@pytest.mark.parametrize("driver", ["cpp", "python"])
+def test_until_l1_stops_where_the_reference_loop_stops(tmp_path, driver):
+    """`while (L1 > limL1)` with a check every 50 steps (quasi.cpp:1014,
+    1969-2029): with a threshold between the reference's 2nd and 3rd L1 of
+    the 64x64x128 run, the loop ends after the 3rd check (step 150).  Also
+    the reference's 6-digit text dumps (--digits 6) and its info header."""
+    z = np.load(GOLDEN / f"{CONFIG1}.npz")
+    meta = json.loads(str(z["meta"]))
+    l1_ref = z["L1"]
+    assert l1_ref[1] > 0.084 >= l1_ref[2]
+    out = tmp_path / "run"
+    argv = ["1", "675", "6", "0", "--ic", "planar", "--seed", str(meta["seed"]), "--grid", str(meta["nx"]),
+            str(meta["ny"]), str(meta["nz"]), "--ranks", str(meta["ranks"]), "--step-l1", "50", "--step-save",
+            "1000", "--until-l1", "0.084", "--digits", "6", "--out", str(out)]
+    cmd = [str(ROOT / "smaiso_quasi_b200" / "quasi_run")] if driver == "cpp" else \
+        [sys.executable, "-m", "smaiso_quasi_b200.run"]
+    r = subprocess.run(cmd + argv, capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert r.returncode == 0, r.stderr
+    assert "150 steps" in r.stdout, r.stdout
+    lines = (out / "L1.dat").read_text().split()
+    assert len(lines) == 3
+    for s in lines:   # 6 significant digits, as the reference's default ostream writes
+        assert len(s.replace(".", "").replace("-", "").split("e")[0].lstrip("0")) <= 6, s
+    np.testing.assert_allclose([float(s) for s in lines], l1_ref[:3], rtol=5e-6)
+    info = (out / "info").read_text()
+    assert "Nx: 64" in info and "stepL1: 50" in info

@@ -7,8 +7,9 @@ from oracle import quasi_oracle as qo
 
 pytestmark = pytest.mark.gpu
 
+# N = 256 on each axis (the headline grid) among them: (256, 16, 32), (16, 256, 32)
 GRIDS = [(16, 16, 32), (8, 16, 16), (32, 64, 16), (96, 96, 192), (64, 64, 128), (128, 32, 256), (512, 16, 32),
-         (16, 32, 512)]
+         (16, 32, 512), (256, 16, 32), (16, 256, 32)]
 
 
 def rel(a, b):
@@ -27,8 +28,9 @@ def test_r2r_fp64_matches_fftw_kinds(grid, plan):
     assert rel(got, ref) < 1e-14
 
 
-@pytest.mark.parametrize("grid", [(16, 16, 32), (64, 64, 128), (96, 96, 192), (16, 32, 512)])
-@pytest.mark.parametrize("plan", ["CT", "iCT", "STx", "iSTz"])
+@pytest.mark.parametrize("grid", [(16, 16, 32), (64, 64, 128), (96, 96, 192), (16, 32, 512), (256, 16, 32),
+                                  (16, 256, 32)])
+@pytest.mark.parametrize("plan", ["CT", "iCT", "STx", "iSTy", "iSTz"])
 def test_r2r_fp32_error(grid, plan):
     import smaiso_quasi_b200 as q
     rng = np.random.default_rng(3)

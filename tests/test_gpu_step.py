@@ -86,10 +86,9 @@ def test_step_fp64_crosses_divv_and_pressure_switches():
         compare(sim, o, 1e-11)
 
 
-@pytest.mark.parametrize("grid", [(32, 32, 64), (24 * 4, 24 * 4, 24 * 8), (16, 16, 512)])
+@pytest.mark.parametrize("grid", [(32, 32, 64), (96, 96, 192), (16, 16, 512), (256, 256, 32), (32, 256, 256)])
 def test_step_fp64_larger_grids(grid):
-    if grid[0] == 96:
-        grid = (96, 96, 192)
+    """Includes N = 256 on x and y (the headline grid's transform lengths)."""
     sim, o = make_pair("quasi", grid, ranks=2)
     for _ in range(3):
         o.step()
@@ -108,7 +107,11 @@ def test_step_stb_matches_oracle():
             assert abs(sim.growth_rate() - o.growth_rate()) <= 1e-9 * abs(o.growth_rate())
 
 
-@pytest.mark.parametrize("name", sorted(p.stem for p in GOLDEN.glob("quasi_*.npz")))
+def _full_fixtures():
+    return sorted(p.stem for p in GOLDEN.glob("quasi_*.npz") if "psi" in np.load(p).files)
+
+
+@pytest.mark.parametrize("name", _full_fixtures())
 def test_step_matches_reference_dumps(name):
     """GPU against the reference's own 17-digit dumps (no oracle in between)."""
     import smaiso_quasi_b200 as q
@@ -131,10 +134,53 @@ def test_step_matches_reference_dumps(name):
     assert len(got["vx"]) == nsl
 
 
-def test_fp32_error_vs_fp64():
-    """The FP32 form against the FP64 form on the same GPU after 50 steps."""
+def test_config1_matches_reference_500_steps():
+    """The 64x64x128 planar interface as the reference runs it with 4 MPI
+    ranks: 500 steps, diagnostics every 50 steps and a mid-slice dump every
+    second diagnostic (quasi.cpp:1969-2280), against the reference's own
+    17-digit dumps."""
     import smaiso_quasi_b200 as q
-    grid = (32, 32, 64)
+    z = np.load(GOLDEN / "quasi_64x64x128_np4_s500.npz")
+    meta = json.loads(str(z["meta"]))
+    grid = (meta["nx"], meta["ny"], meta["nz"])
+    cfg = q.default_config("quasi", *grid, emulate_ranks=meta["ranks"])
+    sim = q.Simulation(cfg)
+    sim.set_psi(q.initial_condition(cfg, meta["ic"], seed=meta["seed"]))
+    sim.init()
+    mid = lambda f: sim.field(f)[:, grid[1] // 2, :].reshape(-1)
+    diags, psi_mid = [], []
+    for s in range(1, meta["steps"] // meta["step_l1"] + 1):
+        sim.step(meta["step_l1"])
+        diags.append(sim.diagnostics())
+        if s % meta["step_save"] == 0:   # a dump every step_save diagnostics (quasi.cpp:2037)
+            psi_mid.append(mid("psi"))
+    d = np.array(diags)
+    np.testing.assert_allclose(d[:, 0], z["L1"], rtol=1e-10)
+    np.testing.assert_allclose(d[:, 1], z["mass"], rtol=1e-12)
+    np.testing.assert_allclose(d[:, 2], z["energy"], rtol=1e-11)
+    assert len(psi_mid) == len(z["psiMid"])
+    for got, ref in zip(psi_mid, z["psiMid"]):
+        assert rel(got, ref) < TOL64
+    got = {f: mid(f) for f in ("vx", "vy", "vz", "rho", "p", "divv")}
+    assert rel(got["rho"], z["rho"][-1]) < TOL64
+    assert rel(got["p"], z["p"][-1]) < 1e-10
+    assert rel(got["divv"], z["divv"][-1]) < 1e-10
+    # 300 steps past the divv switch the difference quotient has amplified
+    # round-off: the oracle itself is 1.9e-11 from these dumps in v
+    assert vec_err(got, {f: z[f][-1] for f in ("vx", "vy", "vz")}) < 1e-10
+
+
+# The FP32 form's tolerance against the FP64 form: 1e-5 relative L2 in psi,
+# rho and the velocity vector.
+TOL32 = 1e-5
+
+
+@pytest.mark.parametrize("grid", [(32, 32, 64), (64, 64, 128)])
+def test_fp32_error_vs_fp64_past_divv_switch(grid):
+    """The FP32 form against the FP64 form on the same GPU after 320 steps,
+    past the divv switch (step 200) where the difference quotient
+    (rho - rho_old)/dt amplifies any rounding noise in rho."""
+    import smaiso_quasi_b200 as q
     cfg64 = q.default_config("quasi", *grid)
     cfg32 = q.default_config("quasi", *grid, precision="fp32")
     psi0 = q.initial_condition(cfg64, "planar", seed=5)
@@ -143,10 +189,12 @@ def test_fp32_error_vs_fp64():
         s = q.Simulation(cfg)
         s.set_psi(psi0)
         s.init()
-        s.step(50)
+        s.step(320)
         sims.append(s)
-    e_psi = rel(sims[1].field("psi"), sims[0].field("psi"))
-    assert e_psi < 1e-5, e_psi
+    a, b = sims[1], sims[0]
+    errs = {"psi": rel(a.field("psi"), b.field("psi")), "rho": rel(a.field("rho"), b.field("rho")),
+            "v": vec_err({f: a.field(f) for f in ("vx", "vy", "vz")}, {f: b.field(f) for f in ("vx", "vy", "vz")})}
+    assert all(v < TOL32 for v in errs.values()), errs
 
 
 def test_checkpoint_round_trip(tmp_path):
