@@ -49,9 +49,16 @@ enum quasi_variant {
 };
 
 enum quasi_precision {
-  QUASI_PREC_FP64 = 0, /* plain form: every field and transform in double */
-  QUASI_PREC_FP32 = 1  /* fields and transforms in float; constants, the
-                          semi-implicit update and reductions in double */
+  QUASI_PREC_FP64 = 0,     /* plain form: every field and transform in double */
+  QUASI_PREC_FP32 = 1,     /* fields and transforms in float; in double: the
+                              carried state psi^, psi, grad psi, the density
+                              chain (law, filter, rho, divv quotient),
+                              constants, the update and the reductions */
+  QUASI_PREC_BF16X3_TC = 2 /* the FP32 form with its plain x / y transforms of
+                              length 256 as split-BF16 (three-product)
+                              contractions on the tensor cores, FP32
+                              accumulation; r2r plans: x / y on the tensor
+                              cores, z by FFT */
 };
 
 enum quasi_field {

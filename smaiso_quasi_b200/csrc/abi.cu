@@ -46,7 +46,8 @@ std::string validate_config(const quasi_config& c) {
   if (c.nz % 16 != 0) return "nz must be a multiple of 16";
   if ((long)c.nx * c.ny % 16 != 0) return "nx*ny must be a multiple of 16";
   if (c.variant != QUASI_VARIANT_QUASI && c.variant != QUASI_VARIANT_STB) return "unknown variant";
-  if (c.precision != QUASI_PREC_FP64 && c.precision != QUASI_PREC_FP32) return "unknown precision";
+  if (c.precision != QUASI_PREC_FP64 && c.precision != QUASI_PREC_FP32 && c.precision != QUASI_PREC_BF16X3_TC)
+    return "unknown precision";
   if (c.emulate_ranks < 1 || c.nx % c.emulate_ranks != 0) return "emulate_ranks must divide nx";
   if (c.emulate_ranks > 1 && c.emulate_ranks % 2 != 0)
     return "emulate_ranks must be 1 or even (the reference's halo exchanges need an even rank count)";
@@ -105,7 +106,7 @@ int quasi_create(const quasi_config* cfg, quasi_handle** out) {
   if (rc) return rc;
   std::string err;
   quasi::EngineBase* e = cfg->precision == QUASI_PREC_FP64 ? quasi::make_engine_f64(*cfg, err)
-                                                           : quasi::make_engine_f32(*cfg, err);
+                                                           : quasi::make_engine_f32(*cfg, err);   // FP32, BF16X3_TC
   if (!e) return fail(err.find("allocation") != std::string::npos ? QUASI_ERR_NOMEM : QUASI_ERR_CUDA, err);
   *out = new (std::nothrow) quasi_handle{e, *cfg};
   if (!*out) {

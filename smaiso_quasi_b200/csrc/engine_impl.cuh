@@ -83,6 +83,7 @@ class Engine : public EngineBase {
       cudaFree(dslab_);
     }
     for (auto& t : tw64_) t.release();
+    if (tc_owned_) cudaFree(tc_owned_);
     if (tma_err_) cudaFree(tma_err_);
     if (tabs_) cudaFree(tabs_);
     if (nloop_dev_) cudaFree(nloop_dev_);
@@ -143,6 +144,10 @@ class Engine : public EngineBase {
     for (int a = 0; a < 3; ++a)
       if (!cuda_ok(tw_[a].upload(len[a]), "twiddles")) return QUASI_ERR_CUDA;
     for (int a = 0; a < 3; ++a) tb_.t[a] = tw_[a].tables();
+    if (cfg_.precision == QUASI_PREC_BF16X3_TC) {   // the tensor-core form's matrices
+      if (!cuda_ok(tc::upload_tables(tc_tables_, &tc_owned_), "contraction matrices")) return QUASI_ERR_CUDA;
+      tc_on_ = true;
+    }
     if constexpr (kStateCopy<T>) {   // the double transforms' own tables
       for (int a = 0; a < 3; ++a)
         if (!cuda_ok(tw64_[a].upload(len[a]), "twiddles")) return QUASI_ERR_CUDA;
@@ -461,6 +466,7 @@ class Engine : public EngineBase {
     t.err = tma_err_;
     t.sms = sms_;
     t.enabled = true;
+    t.tc = tc_on_ ? &tc_tables_ : nullptr;
   }
 
   bool cuda_ok(cudaError_t e, const char* what) {
@@ -580,6 +586,9 @@ class Engine : public EngineBase {
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
   void* slab_ = nullptr;
   double* dslab_ = nullptr;   // the double fields
+  tc::Tables4 tc_tables_{};   // split-BF16 form: the folded DCT/DST matrices
+  void* tc_owned_ = nullptr;
+  bool tc_on_ = false;
   double* tabs_ = nullptr;
   int* nloop_dev_ = nullptr;
   double* partial_ = nullptr;

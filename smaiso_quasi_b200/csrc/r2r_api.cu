@@ -19,6 +19,9 @@ struct R2RBase {
   int sms = 148;
   int inject_skip = -1;             // fault injection for the next execution
   uint32_t inject_polls = kTmaPollLimit;
+  tc::Tables4 tc_tables{};   // the tensor-core form's matrices (precision BF16X3_TC)
+  void* tc_owned = nullptr;
+  bool tc_on = false;
   void use_tma() {
     TmaConfig& t = tma_config();
     t.err = tma_err;
@@ -26,9 +29,11 @@ struct R2RBase {
     t.enabled = true;
     t.skip_tile = inject_skip;
     t.poll_limit = inject_polls;
+    t.tc = tc_on ? &tc_tables : nullptr;
   }
   void end_tma() {   // the injection lasts one execution
     TmaConfig& t = tma_config();
+    t.tc = nullptr;
     t.skip_tile = inject_skip = -1;
     t.poll_limit = inject_polls = kTmaPollLimit;
   }
@@ -50,6 +55,7 @@ struct R2R : R2RBase {
   ~R2R() override {
     cudaSetDevice(device);
     for (auto& t : tw) t.release();
+    if (tc_owned) cudaFree(tc_owned);
     if (own) cudaStreamDestroy(own);
     if (tma_err) cudaFree(tma_err);
   }
@@ -126,6 +132,10 @@ int quasi_r2r_plan_create(int nx, int ny, int nz, const int kind[3], int precisi
     p->nx = nx; p->ny = ny; p->nz = nz; p->device = device; p->elem = 4;
     for (int a = 0; a < 3; ++a) p->kind[a] = kind[a];
     e = p->setup();
+    if (e == cudaSuccess && precision == QUASI_PREC_BF16X3_TC) {
+      e = quasi::tc::upload_tables(p->tc_tables, &p->tc_owned);
+      p->tc_on = true;
+    }
     b = p;
   }
   if (e != cudaSuccess) {

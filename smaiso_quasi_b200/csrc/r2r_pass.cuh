@@ -17,6 +17,7 @@
 #include <type_traits>
 
 #include "r2r_core.cuh"
+#include "tc_pass.cuh"
 #include "tma.cuh"
 
 namespace quasi {
@@ -607,6 +608,7 @@ struct TmaConfig {
   int* err = nullptr;     // device flag, nonzero after a timed-out wait
   uint32_t poll_limit = kTmaPollLimit;   // polls before a tile wait gives up
   int skip_tile = -1;     // fault injection: a tile whose copy is never issued
+  const tc::Tables4* tc = nullptr;   // split-BF16 form: plain float x / y passes on the tensor cores
   int sms = 148;          // CTAs per SM x SMs bounds the persistent grid
   bool enabled = true;
 };
@@ -705,6 +707,13 @@ cudaError_t launch_pass(const Geom& g, int kind, Tables<T> tb, LoadField<T> ld, 
                         int ks = 0) {
   const int n = AXIS == 0 ? g.nx : (AXIS == 1 ? g.ny : g.nz);
   const long extent = AXIS == 2 ? long(g.nx) * g.ny : long(g.nz);
+  if constexpr (std::is_same<T, float>::value && AXIS != 2 && IsStoreField<Store>::value) {
+    if (tma_config().tc && !ks) {
+      const cudaError_t e = tc::launch_tc_pass(g.nx, g.ny, g.nz, AXIS, kind, *tma_config().tc, ld.src, st.dst,
+                                               tma_config().err, tma_config().sms, s);
+      if (e != cudaErrorNotSupported) return e;
+    }
+  }
   if (tma_config().enabled && tma_config().err) {
 #define QUASI_TMA_CASE(NN)                                                                             \
     case NN: {                                                                                         \

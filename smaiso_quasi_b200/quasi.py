@@ -20,7 +20,7 @@ _PKG = pathlib.Path(__file__).resolve().parent
 LIB_PATH = _PKG / "libquasi_gpu.so"
 
 VARIANT = {"quasi": 0, "stb": 1}
-PRECISION = {"fp64": 0, "fp32": 1}
+PRECISION = {"fp64": 0, "fp32": 1, "bf16x3": 2}
 FIELD = {"psi": 0, "rho": 1, "vx": 2, "vy": 3, "vz": 4, "p": 5, "divv": 6, "psiq": 7, "psiq_old": 8,
          "dtpsi": 9, "df": 10}
 KIND = {"REDFT10": 0, "REDFT01": 1, "RODFT10": 2, "RODFT01": 3}

@@ -47,3 +47,22 @@ def test_r2r_round_trip_scale():
     a = np.random.default_rng(5).standard_normal(g)
     b = q.R2RPlan(*g, "iCT").execute_host(q.R2RPlan(*g, "CT").execute_host(a)) * (0.125 / np.prod(g))
     assert rel(b, a) < 1e-14
+
+
+# Split-BF16 tensor-core form: x and y of length 256 as contractions with the
+# folded DCT/DST matrices (three BF16 products, FP32 accumulation), z by FFT.
+# Each contraction pass keeps ~17 significant bits: bound 5e-5 relative L2
+# for the 3-D transform.
+TOL_TC = 5e-5
+
+
+@pytest.mark.parametrize("grid", [(256, 16, 64), (16, 256, 64), (256, 256, 64), (256, 8, 16)])
+@pytest.mark.parametrize("plan", sorted(qo.PLAN_KINDS))
+def test_r2r_bf16x3_tensor_core(grid, plan):
+    import smaiso_quasi_b200 as q
+    rng = np.random.default_rng(11)
+    a = rng.standard_normal(grid)
+    ref = qo.r2r3d(a, qo.PLAN_KINDS[plan])
+    got = q.R2RPlan(*grid, plan, precision="bf16x3").execute_host(a)
+    err = rel(got, ref)
+    assert err < TOL_TC, err
