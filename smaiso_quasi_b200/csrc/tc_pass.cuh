@@ -26,16 +26,18 @@
 //     previous tile's accumulators (tcgen05.ld) and store its outputs.
 // No cluster, no multicast: one CTA's own shared memory and tensor memory.
 #pragma once
-#include <cuda_bf16.h>
-#include <cuda_runtime.h>
-
 #include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <vector>
 
 #include "r2r_core.cuh"
+#ifdef __CUDACC__
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
 #include "tma.cuh"
+#endif
 
 namespace quasi {
 

@@ -51,9 +51,9 @@ def test_r2r_round_trip_scale():
 
 # Split-BF16 tensor-core form: x and y of length 256 as contractions with the
 # folded DCT/DST matrices (three BF16 products, FP32 accumulation), z by FFT.
-# Each contraction pass keeps ~17 significant bits: bound 5e-5 relative L2
+# Each contraction pass is ~3.9e-6 relative L2 (tests/cpu/tc_layout.cpp): bound 2e-5
 # for the 3-D transform.
-TOL_TC = 5e-5
+TOL_TC = 2e-5
 
 
 @pytest.mark.parametrize("grid", [(256, 16, 64), (16, 256, 64), (256, 256, 64), (256, 8, 16)])
