@@ -389,7 +389,7 @@ def main():
                     help="steps after which FP32 is compared with FP64 (default: the workload's run length)")
     ap.add_argument("--workload", default="interface256", choices=sorted(WORKLOADS))
     ap.add_argument("--profile", action="store_true", help="one engine only (for ncu captures)")
-    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"], help="engine of --profile")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64", "bf16x3"], help="engine of --profile")
     ap.add_argument("--axis", type=int, default=1, choices=[0, 1, 2], help="pass timed at the end of --profile")
     args = ap.parse_args()
     global GRID, IC_KIND, METRIC, WORKLOAD

@@ -64,7 +64,7 @@ class Engine : public EngineBase {
   // fields of the storage type (+ the float copies of psiq and rhoq); then
   // the double fields: psiq x 3, rhoq, rho, rho_old, psi x 2, grad psi x 3
   // (+ the scratch of the double transforms in the FP32 form)
-  static constexpr int kFields = 20 + (kStateCopy<T> ? 2 : 0);
+  static constexpr int kFields = 22 + (kStateCopy<T> ? 2 : 0);
   static constexpr int kDFields = 11 + (kStateCopy<T> ? 1 : 0);
   static constexpr int kPhases = 6;   // lcm of the 3-buffer psiq and 2-buffer Nq rotations
 
@@ -158,6 +158,7 @@ class Engine : public EngineBase {
                                     reinterpret_cast<const Cx<double>*>(tb_.t[a].quarter)};
     }
     build_ctx(h);
+    if (!layout_ok_) { err = "internal error: field layout does not match the slab sizes"; return QUASI_ERR_CUDA; }
     // the six step graphs are made here, like the reference's FFTW plans
     // before its loop: quasi_step only launches them
     return capture();
@@ -522,6 +523,8 @@ class Engine : public EngineBase {
     c_.sh = next(); c_.dtpsi = next(); c_.tmp = next();
     if constexpr (kStateCopy<T>) c_.tmp64 = dnext();
     else c_.tmp64 = reinterpret_cast<double*>(c_.tmp);
+    // every field inside its slab (the counts above are the slabs' sizes)
+    layout_ok_ = f == static_cast<T*>(slab_) + size_t(kFields) * n_ && dfp == dslab_ + size_t(kDFields) * n_;
   }
 
   Field field_ptr(int f) const {
@@ -589,6 +592,7 @@ class Engine : public EngineBase {
   tc::Tables4 tc_tables_{};   // split-BF16 form: the folded DCT/DST matrices
   void* tc_owned_ = nullptr;
   bool tc_on_ = false;
+  bool layout_ok_ = false;
   double* tabs_ = nullptr;
   int* nloop_dev_ = nullptr;
   double* partial_ = nullptr;
