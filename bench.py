@@ -357,6 +357,34 @@ def cpu_baseline(samples: int) -> dict | None:
                       f"(FFTW r2r restated, {ranks} MPI ranks as threads), loop wall time"}
 
 
+def run_ensemble(args) -> None:
+    """The batched stability analysis: 48 perturbed planar interfaces
+    (quasi-stb model) on grids drawn from 64^2x128, 96^2x192, 128^2x256, all
+    stepped together (one graph launch per step for the whole ensemble); the
+    FP32 form's growth rates against the same ensemble in FP64."""
+    import numpy as np
+
+    from smaiso_quasi_b200 import ensemble as en
+    members = en.make_members(48, 2024)
+    K = args.steps
+    cells = sum(mb.cells for mb in members)
+    r32 = en.run_members(members, K, "fp32", chunk=K)
+    r64 = en.run_members(members, K, "fp64", chunk=K)
+    g32, g64 = np.array(r32["growth"]), np.array(r64["growth"])
+    rel_err = np.abs(g32 - g64) / np.abs(g64)
+    print(json.dumps({
+        "metric": "instance-steps/s, 48-member stability ensemble (quasi-stb), FP32 form",
+        "value": round(r32["instance_steps_per_s"], 2), "unit": "instance-steps/s", "n_gpus": 1, "steps": K,
+        "warmup": 0, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "48 perturbed planar interfaces, eps log-uniform [0.01, 0.1], m in 1..8, "
+                               "grids from 64^2x128 / 96^2x192 / 128^2x256", "cells": cells,
+                   "timing": "wall clock around quasi_ensemble_step (synchronous) after quasi_ensemble_init"},
+        "cell_updates_per_s": round(r32["cell_updates_per_s"], 1),
+        "fp64": {"instance_steps_per_s": round(r64["instance_steps_per_s"], 2)},
+        "growth_rel_err_vs_fp64": {"max": float(rel_err.max()), "median": float(np.median(rel_err)), "steps": K},
+    }), flush=True)
+
+
 def run_reference(args) -> None:
     rank = int(os.environ.get("RANK", 0))
     if rank != 0:
@@ -387,12 +415,17 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--err-steps", type=int, default=None,
                     help="steps after which FP32 is compared with FP64 (default: the workload's run length)")
-    ap.add_argument("--workload", default="interface256", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="interface256", choices=sorted(WORKLOADS) + ["ensemble48"])
     ap.add_argument("--profile", action="store_true", help="one engine only (for ncu captures)")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64", "bf16x3"], help="engine of --profile")
     ap.add_argument("--axis", type=int, default=1, choices=[0, 1, 2], help="pass timed at the end of --profile")
     args = ap.parse_args()
     global GRID, IC_KIND, METRIC, WORKLOAD
+    if args.workload == "ensemble48":
+        if args.steps is None:
+            args.steps = 200
+        run_ensemble(args)
+        return
     GRID, IC_KIND, METRIC, WORKLOAD, run_len = WORKLOADS[args.workload]
     if args.err_steps is None:
         args.err_steps = run_len

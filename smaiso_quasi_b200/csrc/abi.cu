@@ -195,8 +195,52 @@ int quasi_load(quasi_handle* h, const char* path) {
 // ---------------------------------------------------------------------------
 // Ensembles: a vector of owned handles stepped together.
 // ---------------------------------------------------------------------------
+// The members' step graphs of one rotation phase as child graphs of one
+// graph per phase: when every member is at the same phase on the same device,
+// a step of the whole ensemble is one graph launch (the members' kernels run
+// as independent branches).
 struct quasi_ensemble {
   std::vector<quasi_handle*> members;
+  cudaStream_t stream = nullptr;
+  std::vector<cudaGraphExec_t> exec;   // per phase
+  int device = -1;
+  ~quasi_ensemble() {
+    for (auto& e : exec)
+      if (e) cudaGraphExecDestroy(e);
+    if (stream) cudaStreamDestroy(stream);
+  }
+  // one graph per phase over all members; false if the members do not share
+  // a device or a phase count
+  cudaError_t build(bool* ok) {
+    *ok = false;
+    if (members.empty()) return cudaSuccess;
+    const int dev = members[0]->eng->device(), ph = members[0]->eng->phases();
+    for (auto* h : members)
+      if (h->eng->device() != dev || h->eng->phases() != ph) return cudaSuccess;
+    cudaError_t e = cudaSetDevice(dev);
+    if (e != cudaSuccess) return e;
+    if (!stream && (e = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking)) != cudaSuccess) return e;
+    exec.assign(ph, nullptr);
+    for (int p = 0; p < ph; ++p) {
+      cudaGraph_t g = nullptr;
+      if ((e = cudaGraphCreate(&g, 0)) != cudaSuccess) return e;
+      for (auto* h : members) {
+        cudaGraphNode_t node;
+        cudaGraph_t child = h->eng->phase_graph(p);
+        if (!child) { cudaGraphDestroy(g); return cudaErrorInvalidValue; }
+        if ((e = cudaGraphAddChildGraphNode(&node, g, nullptr, 0, child)) != cudaSuccess) {
+          cudaGraphDestroy(g);
+          return e;
+        }
+      }
+      e = cudaGraphInstantiate(&exec[p], g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) return e;
+    }
+    device = dev;
+    *ok = true;
+    return cudaSuccess;
+  }
 };
 
 namespace {
@@ -253,6 +297,33 @@ int quasi_ensemble_init(quasi_ensemble* e) {
 int quasi_ensemble_step(quasi_ensemble* e, int nsteps) {
   if (!e) return fail(QUASI_ERR_INVALID, "null ensemble");
   if (nsteps < 0) return fail(QUASI_ERR_INVALID, "nsteps < 0");
+  // members in lockstep (initialised, same phase): one graph launch per step
+  bool lockstep = !e->members.empty();
+  const int ph = e->members.empty() ? 1 : e->members[0]->eng->phases();
+  const long phase0 = e->members.empty() ? 0 : e->members[0]->eng->nloop() % ph;
+  for (auto* h : e->members)
+    lockstep = lockstep && h->eng->initialized() && h->eng->phase_graph(0) && h->eng->nloop() % ph == phase0;
+  if (lockstep && e->exec.empty()) {
+    bool ok = false;
+    cudaError_t ce = e->build(&ok);
+    if (ce != cudaSuccess) return fail(QUASI_ERR_CUDA, std::string("ensemble graph: ") + cudaGetErrorString(ce));
+    lockstep = ok;
+  }
+  if (lockstep && !e->exec.empty()) {
+    cudaSetDevice(e->device);
+    for (int s = 0; s < nsteps; ++s) {
+      cudaError_t ce = cudaGraphLaunch(e->exec[(phase0 + s) % ph], e->stream);
+      if (ce != cudaSuccess) return fail(QUASI_ERR_CUDA, std::string("ensemble graph launch: ") + cudaGetErrorString(ce));
+    }
+    cudaError_t ce = cudaStreamSynchronize(e->stream);
+    for (auto* h : e->members) h->eng->note_steps(nsteps);
+    if (ce != cudaSuccess) return fail(QUASI_ERR_CUDA, std::string("ensemble step: ") + cudaGetErrorString(ce));
+    for (size_t m = 0; m < e->members.size(); ++m) {   // each member's wait-timeout flag
+      int rc = quasi_synchronize(e->members[m]);
+      if (rc) return member_fail(m, rc);
+    }
+    return QUASI_OK;
+  }
   // enqueue everything first; then wait for every member (all of them, even
   // after an error, so that no member is left running)
   int first = QUASI_OK;

@@ -33,6 +33,15 @@ class EngineBase {
   virtual long nloop() const = 0;
   virtual int step_kernels(int* n) = 0;
   virtual int time_axis_pass(int axis, int reps, double* avg_ms) = 0;
+  // The captured step graph of rotation phase `ph` (owned by the engine), for
+  // an ensemble that launches all its members' steps as one graph; nullptr
+  // before the graphs exist.
+  virtual cudaGraph_t phase_graph(int ph) const = 0;
+  virtual int phases() const = 0;
+  virtual int device() const = 0;
+  // steps launched for this engine by such a graph (host counter only)
+  virtual void note_steps(int n) = 0;
+  virtual bool initialized() const = 0;
   std::string err;
 };
 

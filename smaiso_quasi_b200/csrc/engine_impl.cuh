@@ -74,6 +74,8 @@ class Engine : public EngineBase {
     if (dev_ok_) cudaSetDevice(cfg_.device);
     for (auto& ge : graph_exec_)
       if (ge) cudaGraphExecDestroy(ge);
+    for (auto& gr : graph_)
+      if (gr) cudaGraphDestroy(gr);
     if (slab_) {
       MapCache::get().forget(slab_, static_cast<char*>(slab_) + size_t(kFields) * n_ * sizeof(T));
       cudaFree(slab_);
@@ -342,6 +344,11 @@ class Engine : public EngineBase {
   }
 
   long nloop() const override { return nloop_; }
+  cudaGraph_t phase_graph(int ph) const override { return graph_[ph]; }
+  int phases() const override { return kPhases; }
+  int device() const override { return cfg_.device; }
+  void note_steps(int n) override { nloop_ += n; }
+  bool initialized() const override { return initialized_; }
 
   int step_kernels(int* n) override {
     if (!graph_exec_[0]) {
@@ -576,7 +583,8 @@ class Engine : public EngineBase {
       if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++graph_kernels_;
     }
     e = cudaGraphInstantiate(&graph_exec_[ph], graph, 0);
-    cudaGraphDestroy(graph);
+    if (graph_[ph]) cudaGraphDestroy(graph_[ph]);
+    graph_[ph] = graph;   // kept for ensembles that launch members as child graphs
     if (!cuda_ok(e, "graph instantiate")) { graph_exec_[ph] = nullptr; return QUASI_ERR_CUDA; }
     return QUASI_OK;
   }
@@ -607,6 +615,7 @@ class Engine : public EngineBase {
   AxisTables<double> tb64_{};
   StepCtx<T> c_{};
   cudaGraphExec_t graph_exec_[kPhases] = {};
+  cudaGraph_t graph_[kPhases] = {};
   double* psiq_buf_[3] = {};
   T* nq_buf_[2] = {};
   double* psi_buf_[2] = {};

@@ -117,7 +117,7 @@ def main(argv=None) -> int:
     ap = argparse.ArgumentParser(prog="python -m smaiso_quasi_b200.ensemble")
     ap.add_argument("--members", type=int, default=48)
     ap.add_argument("--steps", type=int, default=2000)
-    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64", "bf16x3"])
     ap.add_argument("--seed", type=int, default=2024)
     a = ap.parse_args(argv)
     dist = None

@@ -28,26 +28,54 @@ def _entry():
     return q, fn
 
 
-@pytest.mark.parametrize("precision,dtype", [("fp64", "float64"), ("fp32", "float32")])
-def test_noalloc_matches_handle_on_two_calls(precision, dtype):
+@pytest.mark.parametrize("engine", ["fp64", "fp32"])
+def test_noalloc_matches_handle_on_two_calls(engine):
+    """The handle of either form holds psi and rho in double (df in its
+    storage type, exact in double): the fields go in as doubles."""
     import torch
     q, fn = _entry()
-    cfg = q.default_config("quasi", 32, 32, 64, precision=precision)
+    cfg = q.default_config("quasi", 32, 32, 64, precision=engine)
     sim = q.Simulation(cfg)
     sim.set_psi(q.initial_condition(cfg, "planar", seed=3))
     sim.init()
+    dcfg = q.default_config("quasi", 32, 32, 64, precision="fp64")
     for before in (2, 4):            # two calls in a row, at different states
         sim.step(before)
         prev = sim.field("psi")      # psi_old after the next step
         sim.step(1)
         ref = np.array(sim.diagnostics())
         host = [sim.field("psi"), prev, sim.field("rho"), sim.field("df")]
-        dev = [torch.from_numpy(a.astype(dtype)).to("cuda") for a in host]
+        dev = [torch.from_numpy(a).to("cuda") for a in host]
         torch.cuda.synchronize()
         out = (ctypes.c_double * 3)()
-        rc = fn(ctypes.byref(cfg), *[ctypes.c_void_p(t.data_ptr()) for t in dev], out, None)
+        rc = fn(ctypes.byref(dcfg), *[ctypes.c_void_p(t.data_ptr()) for t in dev], out, None)
         assert rc == 0, q.lib().quasi_last_error().decode()
         np.testing.assert_allclose(np.array(out), ref, rtol=RTOL)
+
+
+def test_noalloc_float_fields():
+    """Fields in float (cfg->precision FP32): the FP64 sums over the same float
+    values as the double path computes them."""
+    import torch
+    q, fn = _entry()
+    cfg = q.default_config("quasi", 32, 32, 64, precision="fp32")
+    dcfg = q.default_config("quasi", 32, 32, 64, precision="fp64")
+    sim = q.Simulation(cfg)
+    sim.set_psi(q.initial_condition(cfg, "planar", seed=3))
+    sim.init()
+    sim.step(3)
+    prev = sim.field("psi")
+    sim.step(1)
+    host = [a.astype(np.float32) for a in (sim.field("psi"), prev, sim.field("rho"), sim.field("df"))]
+    outs = []
+    for c, arrs in ((cfg, host), (dcfg, [a.astype(np.float64) for a in host])):
+        dev = [torch.from_numpy(a).to("cuda") for a in arrs]
+        torch.cuda.synchronize()
+        out = (ctypes.c_double * 3)()
+        rc = fn(ctypes.byref(c), *[ctypes.c_void_p(t.data_ptr()) for t in dev], out, None)
+        assert rc == 0, q.lib().quasi_last_error().decode()
+        outs.append(np.array(out))
+    np.testing.assert_allclose(outs[0], outs[1], rtol=RTOL)
 
 
 def test_noalloc_stb_without_df():
