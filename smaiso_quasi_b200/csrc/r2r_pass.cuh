@@ -609,6 +609,7 @@ struct TmaConfig {
   uint32_t poll_limit = kTmaPollLimit;   // polls before a tile wait gives up
   int skip_tile = -1;     // fault injection: a tile whose copy is never issued
   const tc::Tables4* tc = nullptr;   // split-BF16 form: plain float x / y passes on the tensor cores
+  bool zwarp = true;      // z passes of length 64..256 as warp tiles (tma_zpass_warp_kernel)
   int sms = 148;          // CTAs per SM x SMs bounds the persistent grid
   bool enabled = true;
 };

@@ -124,7 +124,7 @@ class MapCache {
   bool lookup(CUtensorMap* out, const void* base, int elem, int nx, int ny, int nz, int axis, const uint32_t box[3]) {
     int dev = 0;
     cudaGetDevice(&dev);
-    auto key = std::make_tuple(dev, base, elem, nx, ny, nz, axis);
+    auto key = std::make_tuple(dev, base, elem, nx, ny, nz, axis, box[0], box[1], box[2]);
     std::lock_guard<std::mutex> lk(mu_);
     auto it = maps_.find(key);
     if (it != maps_.end()) {
@@ -149,7 +149,7 @@ class MapCache {
 
  private:
   std::mutex mu_;
-  std::map<std::tuple<int, const void*, int, int, int, int, int>, CUtensorMap> maps_;
+  std::map<std::tuple<int, const void*, int, int, int, int, int, uint32_t, uint32_t, uint32_t>, CUtensorMap> maps_;
 };
 
 }  // namespace quasi

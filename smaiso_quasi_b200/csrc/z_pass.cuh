@@ -424,6 +424,157 @@ __global__ void __launch_bounds__(256, 2)
   if (tid == 0) bulk_wait0();
 }
 
+// ---------------------------------------------------------------------------
+// Warp-tile z pass: every warp is an independent pipeline over its own tiles
+// of 2G rows (G complex pencils: 2 in float, 1 in double).  It loads its rows
+// with its own TMA copies (two landing buffers, two mbarriers), runs the tile
+// FFT of ZTile with warp-wide synchronisation only (its padded complex tile
+// is its own), stages the output rows over that tile and stores them with
+// its own TMA store.  No CTA barrier after the set-up: warps never wait for
+// each other, so one warp's FFT overlaps the others' copies.
+// ---------------------------------------------------------------------------
+struct WarpExec {
+  template <class R, class W, class Regs>
+  __device__ __forceinline__ void phase(R&& rd, W&& wr, int tid, Regs& regs, bool mid, bool after) {
+    rd(tid, regs);
+    if (mid) __syncwarp();
+    wr(tid, regs);
+    if (after) __syncwarp();
+  }
+  __device__ __forceinline__ void sync() { __syncwarp(); }
+};
+
+template <typename T> constexpr int zw_pencils() { return sizeof(T) == 4 ? 2 : 1; }
+constexpr int kZwWarps = 8;
+
+template <typename T, int N>
+struct ZwLayout {
+  static constexpr int G = zw_pencils<T>(), R = 2 * G;          // pencils, rows per warp tile
+  using Z = ZTile<T, N, G, 32, 1>;
+  static constexpr int RAW = R * N;                              // elements of one landing buffer
+  static constexpr int WB = int(((Z::cb_bytes() + 127) / 128) * 128);   // work bytes per warp
+  static constexpr size_t raw_bytes() { return size_t(kZwWarps) * 2 * RAW * sizeof(T); }
+  static constexpr size_t smem_bytes() {
+    return raw_bytes() + size_t(kZwWarps) * WB + 2 * kZwWarps * 8 + (zpass_root_copy<T>() ? 3 : 2) * N * sizeof(Cx<T>);
+  }
+  static_assert(size_t(R) * N * sizeof(T) <= size_t(WB), "the staging rows overlay the warp's tile");
+};
+
+template <typename T, int N, int KS>
+__global__ void __launch_bounds__(256, 2)
+    tma_zpass_warp_kernel(const __grid_constant__ CUtensorMap src_map, const __grid_constant__ CUtensorMap dst_map,
+                          Geom g, int kind, Tables<T> tb, int ntiles, int* err, uint32_t polls, int skip) {
+  using L = ZwLayout<T, N>;
+  using Z = typename L::Z;
+  constexpr int G = L::G, R = L::R, RAW = L::RAW;
+  constexpr bool kRootCopy = zpass_root_copy<T>();
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  T* raw = reinterpret_cast<T*>(smem_raw) + size_t(warp) * 2 * RAW;   // this warp's landing buffers
+  unsigned char* work_base = smem_raw + L::raw_bytes();
+  Cx<T>* cb = reinterpret_cast<Cx<T>*>(work_base + size_t(warp) * L::WB);
+  T* stg = reinterpret_cast<T*>(cb);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(work_base + size_t(kZwWarps) * L::WB);
+  uint64_t* bar = bars + 2 * warp;
+  Cx<T>* tw1 = reinterpret_cast<Cx<T>*>(bars + 2 * kZwWarps);
+  Cx<T>* qt = tw1 + N;
+  Cx<T>* rt = qt + N;
+  {
+    constexpr int M = N / Z::R1;
+    for (int e = tid; e < N; e += 256) {
+      const int u = e / M, b = e - u * M;
+      tw1[e] = tb.root[b * u];
+      qt[e] = tb.quarter[e];
+      if constexpr (kRootCopy) rt[e] = tb.root[e];
+    }
+    tb.quarter = qt;
+    if constexpr (kRootCopy) tb.root = rt;
+  }
+  if (lane == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();   // tables and barriers ready: the only CTA-wide barrier
+  const int w0 = int(blockIdx.x) * kZwWarps + warp, nwarps = int(gridDim.x) * kZwWarps;
+  auto origin = [&](int t, int& c1, int& c2) {
+    const int row = t * R;   // R rows of one x plane (R divides ny)
+    c2 = row / g.ny;
+    c1 = row - c2 * g.ny;
+  };
+  auto issue = [&](int b, int t) {
+    int c1, c2;
+    origin(t, c1, c2);
+    mbar_expect_tx(&bar[b], uint32_t(RAW * sizeof(T)));
+    tma_load_3d(raw + b * RAW, &src_map, &bar[b], 0, c1, c2);
+  };
+  if (lane == 0) {
+    if (w0 < ntiles && w0 != skip) issue(0, w0);
+    if (w0 + nwarps < ntiles && w0 + nwarps != skip) issue(1, w0 + nwarps);
+  }
+  WarpExec ex;
+  int it = 0;
+  for (int t = w0; t < ntiles; t += nwarps, ++it) {
+    const int b = it & 1;
+    const bool arrived = mbar_wait_bounded(&bar[b], (it >> 1) & 1, polls);
+    if (!__all_sync(0xffffffffu, arrived)) {
+      if (lane == 0) atomicExch(err, 1);
+      const int t_other = t + nwarps;   // drain the other buffer's copy
+      if (t_other < ntiles && t_other != skip) mbar_wait_bounded(&bar[b ^ 1], ((it + 1) >> 1) & 1, polls);
+      break;
+    }
+    typename Z::template Regs<Z::R1> r1;
+    Z::first_read(lane, typename Z::template RowsK<KS>{raw + b * RAW}, kind, tb, r1, tw1);
+    if (lane == 0) bulk_wait_read0();   // the previous store has read the staging rows
+    __syncwarp();
+    const int tn = t + 2 * nwarps;
+    if (lane == 0 && tn < ntiles && tn != skip) {
+      fence_proxy_async_smem();
+      issue(b, tn);
+    }
+    Z::template stage_write<Z::R1, 1>(lane, cb, r1);
+    __syncwarp();
+    ztile_after_first<T, N, G, 32, 1>(ex, lane, kind, cb, stg, tb);
+    fence_proxy_async_smem();
+    __syncwarp();
+    if (lane == 0) {
+      int c1, c2;
+      origin(t, c1, c2);
+      tma_store_3d(&dst_map, stg, 0, c1, c2);
+      bulk_commit();
+    }
+  }
+  if (lane == 0) bulk_wait0();
+}
+
+template <typename T, int N, int KS>
+cudaError_t launch_zpass_warp(const Geom& g, int kind, Tables<T> tb, const T* src, T* dst, cudaStream_t s) {
+  using L = ZwLayout<T, N>;
+  if (g.ny % L::R != 0) return cudaErrorNotSupported;
+  const uint32_t box[3] = {uint32_t(N), uint32_t(L::R), 1};
+  CUtensorMap smap, dmap;
+  if (!MapCache::get().lookup(&smap, src, int(sizeof(T)), g.nx, g.ny, g.nz, 2, box) ||
+      !MapCache::get().lookup(&dmap, dst, int(sizeof(T)), g.nx, g.ny, g.nz, 2, box))
+    return cudaErrorNotSupported;
+  const size_t smem = L::smem_bytes();
+  auto kern = tma_zpass_warp_kernel<T, N, KS>;
+  static int per_sm = 0;   // per instantiation
+  if (per_sm == 0) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return e;
+    int n = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, 256, smem);
+    if (e != cudaSuccess) return e;
+    per_sm = n > 0 ? n : 1;
+  }
+  const int tiles = (g.nx * g.ny) / L::R;
+  const int warps = per_sm * tma_config().sms * kZwWarps;
+  const int grid = tiles < warps ? (tiles + kZwWarps - 1) / kZwWarps : per_sm * tma_config().sms;
+  kern<<<grid, 256, smem, s>>>(smap, dmap, g, kind, tb, tiles, tma_config().err, tma_config().poll_limit,
+                               tma_config().skip_tile);
+  return cudaGetLastError();
+}
+
 #ifndef QUASI_ZPASS
 #define QUASI_ZPASS 1
 #endif
@@ -459,6 +610,13 @@ cudaError_t launch_zpass_nk(const Geom& g, int kind, Tables<T> tb, const T* src,
 
 template <typename T, int N>
 cudaError_t launch_zpass_n(const Geom& g, int kind, Tables<T> tb, const T* src, T* dst, cudaStream_t s, int ks) {
+  if constexpr (N >= 64 && N <= 256) {
+    if (tma_config().zwarp) {
+      const cudaError_t e = ks ? launch_zpass_warp<T, N, 1>(g, kind, tb, src, dst, s)
+                               : launch_zpass_warp<T, N, 0>(g, kind, tb, src, dst, s);
+      if (e != cudaErrorNotSupported) return e;
+    }
+  }
   return ks ? launch_zpass_nk<T, N, 1>(g, kind, tb, src, dst, s) : launch_zpass_nk<T, N, 0>(g, kind, tb, src, dst, s);
 }
 

@@ -126,6 +126,14 @@ template <typename T, int N, int G, int SUB = 1> void ztiles() {
   printf("ztile %s %d %.3g\n", sizeof(T) == 8 ? "f64" : "f32", N * 10 + SUB, w);
 }
 
+// the warp tiles of the z pass: one warp (32 threads) on 2 float or 1 double pencils
+template <typename T, int N> void zwtiles() {
+  constexpr int G = sizeof(T) == 4 ? 2 : 1;
+  double w = 0;
+  for (int k = 0; k < 4; k++) w = std::max({w, ztile_case<T, N, G, 32>(k, 0), ztile_case<T, N, G, 32>(k, 1)});
+  printf("zwtile %s %d %.3g\n", sizeof(T) == 8 ? "f64" : "f32", N, w);
+}
+
 int main() {
   tiles<double, 8, 8, 128>(); tiles<double, 16, 8, 256>(); tiles<double, 32, 8, 128>(); tiles<double, 64, 8, 256>();
   tiles<double, 96, 8, 256>(); tiles<double, 128, 8, 256>(); tiles<double, 192, 8, 256>(); tiles<double, 256, 8, 256>();
@@ -135,5 +143,7 @@ int main() {
   ztiles<float, 16, 16>(); ztiles<float, 64, 16>(); ztiles<float, 96, 16>(); ztiles<float, 128, 16>();
   ztiles<float, 192, 16>(); ztiles<float, 256, 16>();
   ztiles<double, 512, 4, 2>(); ztiles<float, 512, 8, 2>();   // two 256-element blocks per row
+  zwtiles<double, 64>(); zwtiles<double, 96>(); zwtiles<double, 128>(); zwtiles<double, 192>(); zwtiles<double, 256>();
+  zwtiles<float, 64>(); zwtiles<float, 96>(); zwtiles<float, 128>(); zwtiles<float, 192>(); zwtiles<float, 256>();
   return 0;
 }
