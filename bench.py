@@ -226,7 +226,8 @@ def run_gpu(args) -> None:
     cfg32, s32 = make_sim(q, "fp32", device)
     cfg64, s64 = make_sim(q, "fp64", device)
     # the split-BF16 tensor-core form (plain x / y passes as contractions)
-    cfg16, s16 = make_sim(q, "bf16x3", device)
+    cfg16 = q.default_config("quasi", *GRID, precision="bf16x3", device=device, autotune=0)   # the form as such
+    s16 = q.Simulation(cfg16)
     psi0 = q.initial_condition(cfg32, IC_KIND, seed=1234)
 
     # ---- e2e through the public C ABI, host buffers, copies inside ----------
@@ -322,6 +323,7 @@ def run_gpu(args) -> None:
             "bf16x3": {"steps_per_s": round(args.gpus * K / (ms16 / 1e3), 3), "ms_per_step": round(ms16 / K, 4),
                        "err_vs_fp64": err16,
                        "form": "the FP32 form with its plain x / y passes as split-BF16 tensor-core contractions"},
+            "autotune": {"fp32": s32.tuning(), "fp64": s64.tuning()},
             "speedup_fp32_vs_fp64": round(sps32 / sps64, 3),
             "cell_updates_per_s": round(sps * n_cells, 1),
             "err_vs_fp64": err, "err_tolerance": TOL32,

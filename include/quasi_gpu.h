@@ -96,6 +96,12 @@ typedef struct quasi_config {
   int nw;               /* points per wavelength: dx = 2 pi / (q0 nw)    */
   int divv_switch;      /* divv on after this step, p coupling one later */
   double q_pert;        /* quasi-stb growth-rate probe wavenumber Q       */
+  int autotune;         /* 1 (default): quasi_create times the candidate
+                           kernels of each tunable pass (z pass as CTA or
+                           warp tiles per type; FFT or tensor-core x / y
+                           passes in the BF16X3_TC form) on this grid and
+                           keeps the fastest, remembered per grid and
+                           device for later handles; 0: fixed defaults    */
 } quasi_config;
 
 typedef struct quasi_handle quasi_handle;
@@ -125,6 +131,12 @@ QUASI_API int quasi_step(quasi_handle* h, int nsteps);
 /* As quasi_step, timing the steps with CUDA events on the handle's stream;
  * *device_ms receives the elapsed device time of the nsteps steps. */
 QUASI_API int quasi_step_timed(quasi_handle* h, int nsteps, double* device_ms);
+
+/* The autotuner's choices for this handle: out[0] / out[1] = 1 if float /
+ * double z passes run as warp tiles, out[2] = axes (bit 0 x, bit 1 y) whose
+ * plain float passes run on the tensor cores (BF16X3_TC form), out[3] = 1 if
+ * the choices were measured (0: defaults).  No reference counterpart. */
+QUASI_API int quasi_tuning(const quasi_handle* h, int out[4]);
 
 /* Kernel launches in one step (kernel nodes of the step's CUDA graph; the
  * graph is captured by the first quasi_step).  No reference counterpart. */

@@ -81,6 +81,7 @@ int quasi_config_default(quasi_config* c, int variant, int nx, int ny, int nz) {
   c->nu_arg = 1.0;
   c->divv_switch = 200;            /* quasi.cpp:161 */
   c->q_pert = 0.5;                 /* quasi-stb.cpp:157 */
+  c->autotune = 1;
   if (variant == QUASI_VARIANT_QUASI) {
     c->gamma = 1.0; c->beta = 2.0;                 /* quasi.cpp:183-184 */
     c->amp = 1.34164; c->rho_0 = 0.005; c->kp = 0.5;  /* quasi.cpp:194-196 */
@@ -147,6 +148,12 @@ int quasi_synchronize(quasi_handle* h) { QUASI_CALL(h, h->eng->synchronize()); }
 int quasi_step_timed(quasi_handle* h, int nsteps, double* device_ms) {
   if (!device_ms) return fail(QUASI_ERR_INVALID, "null device_ms");
   QUASI_CALL(h, h->eng->step(nsteps, device_ms));
+}
+
+int quasi_tuning(const quasi_handle* h, int out[4]) {
+  if (!h || !out) return fail(QUASI_ERR_INVALID, "null argument");
+  h->eng->tuning(out);
+  return QUASI_OK;
 }
 
 int quasi_step_count(const quasi_handle* h, long* nloop) {

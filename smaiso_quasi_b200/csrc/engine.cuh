@@ -42,6 +42,7 @@ class EngineBase {
   // steps launched for this engine by such a graph (host counter only)
   virtual void note_steps(int n) = 0;
   virtual bool initialized() const = 0;
+  virtual void tuning(int out[4]) const = 0;
   std::string err;
 };
 

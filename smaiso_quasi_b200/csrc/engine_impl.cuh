@@ -163,7 +163,79 @@ class Engine : public EngineBase {
     if (!layout_ok_) { err = "internal error: field layout does not match the slab sizes"; return QUASI_ERR_CUDA; }
     // the six step graphs are made here, like the reference's FFTW plans
     // before its loop: quasi_step only launches them
+    if (cfg_.autotune) {
+      const int rc = autotune();
+      if (rc) return rc;
+    }
     return capture();
+  }
+
+  // Time each tunable pass's candidate kernels on the scratch fields (zeros)
+  // and keep the fastest: the z pass as CTA or warp tiles, per type; in the
+  // BF16X3 form the plain x and y passes on the tensor cores or by FFT.  The
+  // choices are kept per (device, grid, form) for the handles created later
+  // in the process (an ensemble's members of one grid tune once).
+  int autotune() {
+    static std::mutex mu;
+    static std::map<std::tuple<int, int, int, int, int>, Tuning> cache;
+    const auto key = std::make_tuple(cfg_.device, g_.nx, g_.ny, g_.nz, cfg_.precision);
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      auto it = cache.find(key);
+      if (it != cache.end()) {
+        tune_ = it->second;
+        return QUASI_OK;
+      }
+    }
+    auto time = [&](auto&& launch, float* ms) -> bool {
+      for (int w = 0; w < 2; ++w)
+        if (!cuda_ok(launch(), "autotune")) return false;
+      if (!cuda_ok(cudaEventRecord(ev0_, stream_), "event")) return false;
+      for (int r = 0; r < 8; ++r)
+        if (!cuda_ok(launch(), "autotune")) return false;
+      if (!cuda_ok(cudaEventRecord(ev1_, stream_), "event") || !cuda_ok(cudaEventSynchronize(ev1_), "sync"))
+        return false;
+      return cuda_ok(cudaEventElapsedTime(ms, ev0_, ev1_), "elapsed");
+    };
+    Tuning best = tune_;
+    // z pass, storage type and (FP32 form) double
+    for (int d = 0; d < (kStateCopy<T> ? 2 : 1); ++d) {
+      const int slot = kStateCopy<T> ? d : 1;
+      float ms[2] = {0, 0};
+      for (int v = 0; v < 2; ++v) {
+        tune_.zwarp[slot] = v == 1;
+        use_tma();
+        auto z = [&]() -> cudaError_t {
+          if (d == 0) return launch_zpass<T>(g_, E01, tb_.t[2], c_.tmp, c_.tmp, stream_);
+          return launch_zpass<double>(g_, E01, tb64_.t[2], c_.tmp64, c_.tmp64, stream_);
+        };
+        if (!time(z, &ms[v])) return QUASI_ERR_CUDA;
+      }
+      best.zwarp[slot] = ms[1] < ms[0];
+    }
+    tune_ = best;
+    if (tc_on_) {   // x (bit 0) and y (bit 1) on the tensor cores or by FFT
+      int axes = 0;
+      for (int a = 0; a < 2; ++a) {
+        float ms[2] = {0, 0};
+        for (int v = 0; v < 2; ++v) {
+          tune_.tc_axes = v ? (1 << a) : 0;
+          use_tma();
+          auto p = [&]() -> cudaError_t {
+            if (a == 0) return launch_pass<T, 0>(g_, E01, tb_.t[0], LoadField<T>{g_, c_.tmp}, StoreField<T>{g_, c_.tmp}, stream_);
+            return launch_pass<T, 1>(g_, E01, tb_.t[1], LoadField<T>{g_, c_.tmp}, StoreField<T>{g_, c_.tmp}, stream_);
+          };
+          if (!time(p, &ms[v])) return QUASI_ERR_CUDA;
+        }
+        if (ms[1] < ms[0]) axes |= 1 << a;
+      }
+      best.tc_axes = axes;
+    }
+    best.measured = true;
+    tune_ = best;
+    std::lock_guard<std::mutex> lk(mu);
+    cache.emplace(key, best);
+    return QUASI_OK;
   }
 
   int set_psi(const double* host) override {
@@ -349,6 +421,12 @@ class Engine : public EngineBase {
   int device() const override { return cfg_.device; }
   void note_steps(int n) override { nloop_ += n; }
   bool initialized() const override { return initialized_; }
+  void tuning(int out[4]) const override {
+    out[0] = tune_.zwarp[0];
+    out[1] = tune_.zwarp[1];
+    out[2] = tc_on_ ? tune_.tc_axes : 0;
+    out[3] = tune_.measured;
+  }
 
   int step_kernels(int* n) override {
     if (!graph_exec_[0]) {
@@ -475,6 +553,9 @@ class Engine : public EngineBase {
     t.sms = sms_;
     t.enabled = true;
     t.tc = tc_on_ ? &tc_tables_ : nullptr;
+    t.tc_axes = tune_.tc_axes;
+    t.zwarp[0] = tune_.zwarp[0];
+    t.zwarp[1] = tune_.zwarp[1];
   }
 
   bool cuda_ok(cudaError_t e, const char* what) {
@@ -600,6 +681,12 @@ class Engine : public EngineBase {
   tc::Tables4 tc_tables_{};   // split-BF16 form: the folded DCT/DST matrices
   void* tc_owned_ = nullptr;
   bool tc_on_ = false;
+  // the autotuner's choices (see autotune())
+  struct Tuning {
+    bool zwarp[2] = {false, true};
+    int tc_axes = 3;
+    bool measured = false;
+  } tune_;
   bool layout_ok_ = false;
   double* tabs_ = nullptr;
   int* nloop_dev_ = nullptr;

@@ -30,6 +30,9 @@ struct R2RBase {
     t.skip_tile = inject_skip;
     t.poll_limit = inject_polls;
     t.tc = tc_on ? &tc_tables : nullptr;
+    t.tc_axes = 3;
+    t.zwarp[0] = false;
+    t.zwarp[1] = true;
   }
   void end_tma() {   // the injection lasts one execution
     TmaConfig& t = tma_config();

@@ -609,7 +609,10 @@ struct TmaConfig {
   uint32_t poll_limit = kTmaPollLimit;   // polls before a tile wait gives up
   int skip_tile = -1;     // fault injection: a tile whose copy is never issued
   const tc::Tables4* tc = nullptr;   // split-BF16 form: plain float x / y passes on the tensor cores
-  bool zwarp = true;      // z passes of length 64..256 as warp tiles (tma_zpass_warp_kernel)
+  // z passes of length 64..256 as warp tiles (tma_zpass_warp_kernel) rather
+  // than CTA tiles, for float [0] and double [1] passes
+  bool zwarp[2] = {false, true};
+  int tc_axes = 3;        // with tc: the axes (bit 0 x, bit 1 y) that use it
   int sms = 148;          // CTAs per SM x SMs bounds the persistent grid
   bool enabled = true;
 };
@@ -709,7 +712,7 @@ cudaError_t launch_pass(const Geom& g, int kind, Tables<T> tb, LoadField<T> ld, 
   const int n = AXIS == 0 ? g.nx : (AXIS == 1 ? g.ny : g.nz);
   const long extent = AXIS == 2 ? long(g.nx) * g.ny : long(g.nz);
   if constexpr (std::is_same<T, float>::value && AXIS != 2 && IsStoreField<Store>::value) {
-    if (tma_config().tc && !ks) {
+    if (tma_config().tc && ((tma_config().tc_axes >> AXIS) & 1) && !ks) {
       const cudaError_t e = tc::launch_tc_pass(g.nx, g.ny, g.nz, AXIS, kind, *tma_config().tc, ld.src, st.dst,
                                                tma_config().err, tma_config().sms, s);
       if (e != cudaErrorNotSupported) return e;

@@ -611,7 +611,7 @@ cudaError_t launch_zpass_nk(const Geom& g, int kind, Tables<T> tb, const T* src,
 template <typename T, int N>
 cudaError_t launch_zpass_n(const Geom& g, int kind, Tables<T> tb, const T* src, T* dst, cudaStream_t s, int ks) {
   if constexpr (N >= 64 && N <= 256) {
-    if (tma_config().zwarp) {
+    if (tma_config().zwarp[sizeof(T) == 8]) {
       const cudaError_t e = ks ? launch_zpass_warp<T, N, 1>(g, kind, tb, src, dst, s)
                                : launch_zpass_warp<T, N, 0>(g, kind, tb, src, dst, s);
       if (e != cudaErrorNotSupported) return e;

@@ -37,6 +37,7 @@ EXPORTS = [
     "quasi_r2r_execute_device", "quasi_r2r_execute_host", "quasi_r2r_plan_destroy",
     "quasi_ic_default", "quasi_initial_condition", "quasi_step_kernels", "quasi_time_axis_pass",
     "quasi_step_async", "quasi_synchronize", "quasi_diagnostics_noalloc", "quasi_r2r_inject_wait_timeout",
+    "quasi_tuning",
     "quasi_ensemble_create", "quasi_ensemble_size", "quasi_ensemble_member", "quasi_ensemble_init",
     "quasi_ensemble_step", "quasi_ensemble_growth_rates", "quasi_ensemble_destroy",
 ]
@@ -59,6 +60,7 @@ class Config(ctypes.Structure):
         ("gamma", ctypes.c_double), ("beta", ctypes.c_double), ("alpha", ctypes.c_double), ("q0", ctypes.c_double),
         ("amp", ctypes.c_double), ("rho_0", ctypes.c_double), ("kp", ctypes.c_double), ("rho_m", ctypes.c_double),
         ("dt", ctypes.c_double), ("nw", ctypes.c_int), ("divv_switch", ctypes.c_int), ("q_pert", ctypes.c_double),
+        ("autotune", ctypes.c_int),
     ]
 
 
@@ -107,6 +109,7 @@ def lib() -> ctypes.CDLL:
         L.quasi_r2r_plan_destroy.argtypes = [ctypes.c_void_p]
         L.quasi_r2r_inject_wait_timeout.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_uint]
         L.quasi_step_kernels.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
+        L.quasi_tuning.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
         L.quasi_time_axis_pass.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, dp]
         L.quasi_ic_default.argtypes = [ctypes.POINTER(IC), ctypes.c_int]
         L.quasi_initial_condition.argtypes = [ctypes.POINTER(Config), ctypes.POINTER(IC), dp]
@@ -217,6 +220,13 @@ class Simulation:
         n = ctypes.c_int()
         _check(lib().quasi_step_kernels(self._h, ctypes.byref(n)))
         return n.value
+
+    def tuning(self) -> dict:
+        """The autotuner's choices (quasi_tuning)."""
+        out = (ctypes.c_int * 4)()
+        _check(lib().quasi_tuning(self._h, out))
+        return {"z_warp_tiles_float": bool(out[0]), "z_warp_tiles_double": bool(out[1]),
+                "tensor_core_axes": int(out[2]), "measured": bool(out[3])}
 
     def time_axis_pass(self, axis: int, reps: int = 20) -> float:
         ms = ctypes.c_double()
