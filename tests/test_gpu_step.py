@@ -216,8 +216,9 @@ def test_checkpoint_round_trip(tmp_path):
 
 def test_autotuner_choices_do_not_change_results():
     """quasi_create's autotuner picks among kernels that compute the same
-    arithmetic (CTA or warp tiles of the z pass): a tuned and an untuned
-    handle step to bitwise identical fields."""
+    transform (CTA or warp tiles of the z pass; the compiler may contract
+    their multiply-adds differently): a tuned and an untuned FP32 handle agree
+    to float rounding, and tuning also covers shapes the TMA passes do not."""
     import smaiso_quasi_b200 as q
     out = []
     for tune in (1, 0):
@@ -229,4 +230,6 @@ def test_autotuner_choices_do_not_change_results():
         s.init()
         s.step(5)
         out.append(s.field("psi"))
-    assert np.array_equal(out[0], out[1])
+    assert rel(out[0], out[1]) < 1e-6
+    small = q.Simulation(q.default_config("stb", 16, 16, 32, precision="fp32"))   # no TMA z pass here
+    assert small.tuning()["measured"]
