@@ -173,7 +173,7 @@ class Engine : public EngineBase {
   // Time each tunable pass's candidate kernels on the scratch fields (zeros)
   // and keep the fastest: the z pass as CTA or warp tiles, per type; in the
   // BF16X3 form the plain x and y passes on the tensor cores or by FFT.  The
-  // two candidates are timed in alternation (3 rounds of 6 launches each, the
+  // two candidates are timed in alternation (5 rounds of 10 launches each, the
   // best round of each counts), and the default stays unless the other is
   // faster by more than 3%.  The choices are kept per (device, grid, form) for
   // the handles created later in the process (an ensemble's members of one
@@ -200,7 +200,7 @@ class Engine : public EngineBase {
       }
       if (!cuda_ok(e0, "autotune")) return false;
       if (!cuda_ok(cudaEventRecord(ev0_, stream_), "event")) return false;
-      for (int r = 0; r < 6; ++r)
+      for (int r = 0; r < 10; ++r)
         if (!cuda_ok(launch(), "autotune")) return false;
       if (!cuda_ok(cudaEventRecord(ev1_, stream_), "event") || !cuda_ok(cudaEventSynchronize(ev1_), "sync"))
         return false;
@@ -209,7 +209,7 @@ class Engine : public EngineBase {
     // best[v] over alternating rounds of the two settings applied by set(v)
     auto race = [&](auto&& set, auto&& launch, float best[2]) -> bool {
       best[0] = best[1] = 1e30f;
-      for (int round = 0; round < 3; ++round)
+      for (int round = 0; round < 5; ++round)
         for (int v = 0; v < 2; ++v) {
           set(v);
           use_tma();
