@@ -132,10 +132,11 @@ QUASI_API int quasi_step(quasi_handle* h, int nsteps);
  * *device_ms receives the elapsed device time of the nsteps steps. */
 QUASI_API int quasi_step_timed(quasi_handle* h, int nsteps, double* device_ms);
 
-/* The autotuner's choices for this handle: out[0] / out[1] = 1 if float /
- * double z passes run as warp tiles, out[2] = axes (bit 0 x, bit 1 y) whose
- * plain float passes run on the tensor cores (BF16X3_TC form), out[3] = 1 if
- * the choices were measured (0: defaults).  No reference counterpart. */
+/* The autotuner's choices for this handle: out[0] / out[1] = the float /
+ * double passes that run as warp tiles (bit 0 z, bit 1 x, bit 2 y; the rest as
+ * CTA tiles), out[2] = axes (bit 0 x, bit 1 y) whose plain float passes run on
+ * the tensor cores (BF16X3_TC form), out[3] = 1 if the choices were measured
+ * (0: defaults).  No reference counterpart. */
 QUASI_API int quasi_tuning(const quasi_handle* h, int out[4]);
 
 /* Kernel launches in one step (kernel nodes of the step's CUDA graph; the

@@ -240,6 +240,27 @@ class Engine : public EngineBase {
       if (!race([&](int v) { tune_.zwarp[slot] = v == 1; }, z, ms)) return QUASI_ERR_CUDA;
       best.zwarp[slot] = better(ms, Tuning{}.zwarp[slot]);
       tune_ = best;
+      // x and y passes as CTA or warp tiles (the plain pass decides for all
+      // passes of that axis and type)
+      for (int a = 0; a < 2; ++a) {
+        auto xy = [&]() -> cudaError_t {
+          if (d == 0) {
+            if (a == 0) return launch_pass<T, 0>(g_, E01, tb_.t[0], LoadField<T>{g_, c_.tmp}, StoreField<T>{g_, c_.tmp}, stream_);
+            return launch_pass<T, 1>(g_, E01, tb_.t[1], LoadField<T>{g_, c_.tmp}, StoreField<T>{g_, c_.tmp}, stream_);
+          }
+          if (a == 0)
+            return launch_pass<double, 0>(g_, E01, tb64_.t[0], LoadField<double>{g_, c_.tmp64},
+                                          StoreField<double>{g_, c_.tmp64}, stream_);
+          return launch_pass<double, 1>(g_, E01, tb64_.t[1], LoadField<double>{g_, c_.tmp64},
+                                        StoreField<double>{g_, c_.tmp64}, stream_);
+        };
+        const int tc_keep = tune_.tc_axes;
+        tune_.tc_axes = 0;   // the FFT passes are what is tuned here
+        if (!race([&](int v) { tune_.xywarp[a][slot] = v == 1; }, xy, ms)) return QUASI_ERR_CUDA;
+        tune_.tc_axes = tc_keep;
+        best.xywarp[a][slot] = better(ms, false);
+        tune_ = best;
+      }
     }
     if (tc_on_) {   // x (bit 0) and y (bit 1) on the tensor cores or by FFT
       int axes = 0;
@@ -445,8 +466,8 @@ class Engine : public EngineBase {
   void note_steps(int n) override { nloop_ += n; }
   bool initialized() const override { return initialized_; }
   void tuning(int out[4]) const override {
-    out[0] = tune_.zwarp[0];
-    out[1] = tune_.zwarp[1];
+    for (int d = 0; d < 2; ++d)
+      out[d] = int(tune_.zwarp[d]) | (int(tune_.xywarp[0][d]) << 1) | (int(tune_.xywarp[1][d]) << 2);
     out[2] = tc_on_ ? tune_.tc_axes : 0;
     out[3] = tune_.measured;
   }
@@ -579,6 +600,8 @@ class Engine : public EngineBase {
     t.tc_axes = tune_.tc_axes;
     t.zwarp[0] = tune_.zwarp[0];
     t.zwarp[1] = tune_.zwarp[1];
+    for (int a = 0; a < 2; ++a)
+      for (int d = 0; d < 2; ++d) t.xywarp[a][d] = tune_.xywarp[a][d];
   }
 
   bool cuda_ok(cudaError_t e, const char* what) {
@@ -707,6 +730,7 @@ class Engine : public EngineBase {
   // the autotuner's choices (see autotune())
   struct Tuning {
     bool zwarp[2] = {false, true};
+    bool xywarp[2][2] = {{false, false}, {false, false}};   // [axis x, y][float, double]
     int tc_axes = 3;
     bool measured = false;
   } tune_;

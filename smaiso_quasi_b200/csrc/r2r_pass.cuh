@@ -37,6 +37,19 @@ struct DevExec {
   __device__ __forceinline__ void sync() { __syncthreads(); }
 };
 
+// The same phases synchronised within one warp only (warp-tile kernels, whose
+// tiles belong to one warp).
+struct WarpExec {
+  template <class R, class W, class Regs>
+  __device__ __forceinline__ void phase(R&& rd, W&& wr, int tid, Regs& regs, bool mid, bool after) {
+    rd(tid, regs);
+    if (mid) __syncwarp();
+    wr(tid, regs);
+    if (after) __syncwarp();
+  }
+  __device__ __forceinline__ void sync() { __syncwarp(); }
+};
+
 struct Geom {
   int nx, ny, nz;
 };
@@ -568,6 +581,143 @@ __global__ void __launch_bounds__(tma_threads<T>(), 2)
   }
 }
 
+// ---------------------------------------------------------------------------
+// Warp-tile x / y pass: the same tile transform as tma_pass_kernel, but every
+// warp is an independent pipeline over its own tiles of PW = 2 G columns (G
+// complex pencils: 2 in float, 1 in double) x all N rows: its own two landing
+// buffers filled by its own TMA copies (a box PW columns wide, 16 bytes), its
+// own mbarriers, its own work tile, staging rows and TMA stores, and warp-wide
+// synchronisation only.  N <= 256 (one box along the axis).
+// ---------------------------------------------------------------------------
+template <typename T> constexpr int xyw_cols() { return sizeof(T) == 4 ? 4 : 2; }
+constexpr int kXywWarps = 8;
+
+template <typename T, int N>
+struct XywLayout {
+  static constexpr int PW = xyw_cols<T>(), G = PW / 2;
+  static constexpr int RAW = PW * N;                                  // elements of one landing buffer
+  static constexpr int WORK = ((PW * tile_ld(N) + 31) / 32) * 32;    // work tile elements (128-byte multiple)
+  static constexpr size_t per_warp() { return size_t(2 * RAW + WORK) * sizeof(T); }
+  static constexpr size_t smem_bytes() {
+    return size_t(kXywWarps) * per_warp() + 2 * kXywWarps * 8 + 2 * N * sizeof(Cx<T>);
+  }
+  static_assert(RAW <= WORK, "the staging rows overlay the work tile");
+};
+
+template <typename T, int N, int AXIS, class Store, class Mul, class Mul2 = NoMul, bool TSTORE = false>
+__global__ void __launch_bounds__(256, 2)
+    tma_pass_warp_kernel(const __grid_constant__ CUtensorMap map, Geom g, int kind, Tables<T> tb, Store st,
+                         int ntiles, int* err, uint32_t polls, int skip, Mul mul, int dc1, int dc2, Store st2,
+                         Mul2 mul2, const __grid_constant__ CUtensorMap dmap,
+                         const __grid_constant__ CUtensorMap dmap2) {
+  static_assert(AXIS != 2 && N <= 256, "x / y passes of one box along the axis");
+  using L = XywLayout<T, N>;
+  constexpr int PW = L::PW, G = L::G, RAW = L::RAW;
+  constexpr bool kDual = !std::is_same<Mul2, NoMul>::value;
+  static_assert(!TSTORE || !kDual || IsStoreField<Store>::value, "dual passes stage plain fields");
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  T* raw0 = reinterpret_cast<T*>(smem_raw + size_t(warp) * L::per_warp());
+  T* raw1 = raw0 + RAW;
+  T* work = raw1 + RAW;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + size_t(kXywWarps) * L::per_warp());
+  uint64_t* bar = bars + 2 * warp;
+  {
+    Cx<T>* rt = reinterpret_cast<Cx<T>*>(bars + 2 * kXywWarps);
+    Cx<T>* qt = rt + N;
+    for (int e = tid; e < N; e += 256) {
+      rt[e] = tb.root[e];
+      qt[e] = tb.quarter[e];
+    }
+    tb.root = rt;
+    tb.quarter = qt;
+  }
+  if (lane == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();   // tables and barriers ready: the only CTA-wide barrier
+  const int w0 = int(blockIdx.x) * kXywWarps + warp, nw = int(gridDim.x) * kXywWarps;
+  if (lane == 0) {
+    if (w0 < ntiles && w0 != skip) tma_issue_tile<T, N, AXIS, PW>(&map, raw0, &bar[0], g, w0, dc1, dc2);
+    if (w0 + nw < ntiles && w0 + nw != skip) tma_issue_tile<T, N, AXIS, PW>(&map, raw1, &bar[1], g, w0 + nw, dc1, dc2);
+  }
+  WarpExec ex;
+  int it = 0;
+  for (int t = w0; t < ntiles; t += nw, ++it) {
+    const int b = it & 1;
+    T* raw = b ? raw1 : raw0;
+    const bool arrived = mbar_wait_bounded(&bar[b], (it >> 1) & 1, polls);
+    if constexpr (TSTORE) {
+      if (lane == 0) bulk_wait_read0();   // the previous tile's store has read the staging rows
+    }
+    if (!__all_sync(0xffffffffu, arrived)) {
+      if (lane == 0) atomicExch(err, 1);
+      drain_other(bar, b, it, t, nw, ntiles, skip, polls);
+      break;
+    }
+    __syncwarp();
+    const int t_next = t + 2 * nw;
+    auto store_tile = [&](const CUtensorMap* dm) {
+      fence_proxy_async_smem();
+      __syncwarp();
+      if (lane == 0) {
+        int c0, c1, c2;
+        tile_origin<AXIS, PW>(g, t, c0, c1, c2);
+        tma_store_3d(dm, work, c0, c1, c2);
+        bulk_commit();
+      }
+    };
+    auto issue_next = [&]() {
+      if (lane == 0 && t_next < ntiles && t_next != skip) {
+        fence_proxy_async_smem();
+        tma_issue_tile<T, N, AXIS, PW>(&map, raw, &bar[b], g, t_next, dc1, dc2);
+      }
+    };
+    const int kt = g.nz / PW;
+    const int outer = t / kt, k0 = (t - outer * kt) * PW;
+    MulSrc<T, AXIS, Mul> src{raw, PW, outer, k0, mul};
+    src.prep(lane % G);
+    if constexpr (kDual) {
+      if constexpr (TSTORE) {
+        r2r_tile<T, N, G, 32, false>(ex, lane, kind, reinterpret_cast<Cx<T>*>(work), src, RowStageSnk<T>{work, PW}, tb);
+        store_tile(&dmap);
+        if (lane == 0) bulk_wait_read0();
+      } else {
+        r2r_tile<T, N, G, 32, false>(ex, lane, kind, reinterpret_cast<Cx<T>*>(work), src,
+                                     GlobSnk<T, AXIS, Store>{st, outer, k0}, tb);
+      }
+      __syncwarp();   // the second transform rewrites the work tile
+      MulSrc<T, AXIS, Mul2> src2{raw, PW, outer, k0, mul2};
+      src2.prep(lane % G);
+      if constexpr (TSTORE) {
+        r2r_tile<T, N, G, 32, false>(ex, lane, kind, reinterpret_cast<Cx<T>*>(work), src2, RowStageSnk<T>{work, PW}, tb,
+                                     issue_next);
+        store_tile(&dmap2);
+      } else {
+        r2r_tile<T, N, G, 32, false>(ex, lane, kind, reinterpret_cast<Cx<T>*>(work), src2,
+                                     GlobSnk<T, AXIS, Store>{st2, outer, k0}, tb, issue_next);
+      }
+    } else if constexpr (TSTORE && IsStoreField<Store>::value) {
+      r2r_tile<T, N, G, 32, false>(ex, lane, kind, reinterpret_cast<Cx<T>*>(work), src, RowStageSnk<T>{work, PW}, tb,
+                                   issue_next);
+      store_tile(&dmap);
+    } else if constexpr (TSTORE) {
+      r2r_tile<T, N, G, 32, false>(ex, lane, kind, reinterpret_cast<Cx<T>*>(work), src,
+                                   RowStageValSnk<T, AXIS, Store>{work, PW, outer, k0, st}, tb, issue_next);
+      store_tile(&dmap);
+    } else {
+      r2r_tile<T, N, G, 32, false>(ex, lane, kind, reinterpret_cast<Cx<T>*>(work), src,
+                                   GlobSnk<T, AXIS, Store>{st, outer, k0}, tb, issue_next);
+    }
+    __syncwarp();   // the next tile's first stage overwrites `work`
+  }
+  if constexpr (TSTORE) {
+    if (lane == 0) bulk_wait0();
+  }
+}
+
 template <typename T, int N, int P>
 inline size_t tma_smem_bytes() {
   return size_t(2) * P * N * sizeof(T) + size_t(tma_work_elems<T, N, P>()) * sizeof(T) + 16 +
@@ -612,6 +762,8 @@ struct TmaConfig {
   // z passes of length 64..256 as warp tiles (tma_zpass_warp_kernel) rather
   // than CTA tiles, for float [0] and double [1] passes
   bool zwarp[2] = {false, true};
+  // x [0] / y [1] passes as warp tiles (tma_pass_warp_kernel), float / double
+  bool xywarp[2][2] = {{false, false}, {false, false}};
   int tc_axes = 3;        // with tc: the axes (bit 0 x, bit 1 y) that use it
   int sms = 148;          // CTAs per SM x SMs bounds the persistent grid
   bool enabled = true;
@@ -621,10 +773,61 @@ inline TmaConfig& tma_config() {
   return c;
 }
 
+// The warp-tile form of an x / y pass (tma_pass_warp_kernel).
+template <typename T, int N, int AXIS, class Store, class Mul, class Mul2>
+cudaError_t launch_tma_pass_warp(const Geom& g, int kind, Tables<T> tb, const T* src, Store st, cudaStream_t s,
+                                 Mul mul, int dc1, int dc2, Store st2, Mul2 mul2) {
+  using L = XywLayout<T, N>;
+  constexpr int PW = L::PW;
+  if (g.nz % PW != 0) return cudaErrorNotSupported;
+  uint32_t box[3];
+  if (AXIS == 1) { box[0] = PW; box[1] = N; box[2] = 1; }
+  else { box[0] = PW; box[1] = 1; box[2] = N; }
+  CUtensorMap map;
+  if (!MapCache::get().lookup(&map, src, int(sizeof(T)), g.nx, g.ny, g.nz, AXIS, box)) return cudaErrorNotSupported;
+  constexpr bool kStaged = IsStoreField<Store>::value || HasStageValue<Store>::value;
+  constexpr bool TSTORE = kStaged;
+  CUtensorMap dmap = map, dmap2 = map;
+  if constexpr (TSTORE) {
+    const T* dptr;
+    if constexpr (IsStoreField<Store>::value) dptr = st.dst;
+    else dptr = st.stage_dst();
+    if (!MapCache::get().lookup(&dmap, dptr, int(sizeof(T)), g.nx, g.ny, g.nz, AXIS, box))
+      return cudaErrorNotSupported;
+    if constexpr (!std::is_same<Mul2, NoMul>::value) {
+      if (!MapCache::get().lookup(&dmap2, st2.dst, int(sizeof(T)), g.nx, g.ny, g.nz, AXIS, box))
+        return cudaErrorNotSupported;
+    }
+  }
+  const size_t smem = L::smem_bytes();
+  auto kern = tma_pass_warp_kernel<T, N, AXIS, Store, Mul, Mul2, TSTORE>;
+  static int per_sm = 0;   // per instantiation: resident CTAs per SM
+  if (per_sm == 0) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int n = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, 256, smem);
+    if (e != cudaSuccess) return e;
+    per_sm = n > 0 ? n : 1;
+  }
+  const int tiles = (AXIS == 1 ? g.nx : g.ny) * (g.nz / PW);
+  const int full = per_sm * tma_config().sms;
+  const int grid = tiles < full * kXywWarps ? (tiles + kXywWarps - 1) / kXywWarps : full;
+  kern<<<grid, 256, smem, s>>>(map, g, kind, tb, st, tiles, tma_config().err, tma_config().poll_limit,
+                               tma_config().skip_tile, mul, dc1, dc2, st2, mul2, dmap, dmap2);
+  return cudaGetLastError();
+}
+
 template <typename T, int N, int AXIS, int P, class Store, class Mul = NoMul, class Mul2 = NoMul>
 cudaError_t launch_tma_pass(const Geom& g, int kind, Tables<T> tb, const T* src, Store st, cudaStream_t s,
                             Mul mul = Mul(), int dc1 = 0, int dc2 = 0, int ks = 0, Store st2 = Store(),
                             Mul2 mul2 = Mul2()) {
+  if constexpr (AXIS != 2 && N <= 256) {
+    if (tma_config().xywarp[AXIS][sizeof(T) == 8]) {
+      const cudaError_t e = launch_tma_pass_warp<T, N, AXIS>(g, kind, tb, src, st, s, mul, dc1, dc2, st2, mul2);
+      if (e != cudaErrorNotSupported) return e;
+    }
+  }
   uint32_t box[3];
   constexpr int SUB = (N + 255) / 256;
   if (AXIS == 2) { box[0] = N; box[1] = P; box[2] = 1; }

@@ -433,17 +433,6 @@ __global__ void __launch_bounds__(256, 2)
 // its own TMA store.  No CTA barrier after the set-up: warps never wait for
 // each other, so one warp's FFT overlaps the others' copies.
 // ---------------------------------------------------------------------------
-struct WarpExec {
-  template <class R, class W, class Regs>
-  __device__ __forceinline__ void phase(R&& rd, W&& wr, int tid, Regs& regs, bool mid, bool after) {
-    rd(tid, regs);
-    if (mid) __syncwarp();
-    wr(tid, regs);
-    if (after) __syncwarp();
-  }
-  __device__ __forceinline__ void sync() { __syncwarp(); }
-};
-
 template <typename T> constexpr int zw_pencils() { return sizeof(T) == 4 ? 2 : 1; }
 constexpr int kZwWarps = 8;
 

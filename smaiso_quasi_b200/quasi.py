@@ -225,7 +225,9 @@ class Simulation:
         """The autotuner's choices (quasi_tuning)."""
         out = (ctypes.c_int * 4)()
         _check(lib().quasi_tuning(self._h, out))
-        return {"z_warp_tiles_float": bool(out[0]), "z_warp_tiles_double": bool(out[1]),
+        names = ("z", "x", "y")
+        return {"warp_tiles_float": [n for b, n in enumerate(names) if out[0] >> b & 1],
+                "warp_tiles_double": [n for b, n in enumerate(names) if out[1] >> b & 1],
                 "tensor_core_axes": int(out[2]), "measured": bool(out[3])}
 
     def time_axis_pass(self, axis: int, reps: int = 20) -> float:

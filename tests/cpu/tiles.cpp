@@ -126,6 +126,14 @@ template <typename T, int N, int G, int SUB = 1> void ztiles() {
   printf("ztile %s %d %.3g\n", sizeof(T) == 8 ? "f64" : "f32", N * 10 + SUB, w);
 }
 
+// the warp tiles of the x / y passes: one warp (32 threads) on 2 float or 1 double pencils
+template <typename T, int N> void wtiles() {
+  constexpr int G = sizeof(T) == 4 ? 2 : 1;
+  double w = 0;
+  for (int k = 0; k < 4; k++) w = std::max({w, tile_case<T, N, G, 32>(k, true), tile_case<T, N, G, 32>(k, false)});
+  printf("wtile %s %d %.3g\n", sizeof(T) == 8 ? "f64" : "f32", N, w);
+}
+
 // the warp tiles of the z pass: one warp (32 threads) on 2 float or 1 double pencils
 template <typename T, int N> void zwtiles() {
   constexpr int G = sizeof(T) == 4 ? 2 : 1;
@@ -143,6 +151,9 @@ int main() {
   ztiles<float, 16, 16>(); ztiles<float, 64, 16>(); ztiles<float, 96, 16>(); ztiles<float, 128, 16>();
   ztiles<float, 192, 16>(); ztiles<float, 256, 16>();
   ztiles<double, 512, 4, 2>(); ztiles<float, 512, 8, 2>();   // two 256-element blocks per row
+  // the warp tiles of the x / y passes: one warp on 2 float or 1 double pencils
+  wtiles<double, 64>(); wtiles<double, 96>(); wtiles<double, 128>(); wtiles<double, 192>(); wtiles<double, 256>();
+  wtiles<float, 64>(); wtiles<float, 128>(); wtiles<float, 256>();
   zwtiles<double, 64>(); zwtiles<double, 96>(); zwtiles<double, 128>(); zwtiles<double, 192>(); zwtiles<double, 256>();
   zwtiles<float, 64>(); zwtiles<float, 96>(); zwtiles<float, 128>(); zwtiles<float, 192>(); zwtiles<float, 256>();
   return 0;

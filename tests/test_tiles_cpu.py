@@ -1,5 +1,5 @@
 """The tile transforms' index arithmetic on the CPU: the device code of
-r2r_core.cuh (x / y tiles) and z_pass.cuh (z tiles of a CTA and of one warp,
+r2r_core.cuh (x / y tiles of a CTA and of one warp) and z_pass.cuh (z tiles of a CTA and of one warp,
 with and without the one-row shift of the z gradients) compiled for the host and run serially,
 against FFTW's REDFT10/01 and RODFT10/01 definitions in long double."""
 import pathlib
@@ -26,11 +26,12 @@ def results(tmp_path_factory):
 
 def test_every_case_ran(results):
     assert sum(1 for k in results if k[0] == "tile") == 12
+    assert sum(1 for k in results if k[0] == "wtile") == 8
     assert sum(1 for k in results if k[0] == "ztile") == 16
     assert sum(1 for k in results if k[0] == "zwtile") == 10
 
 
-@pytest.mark.parametrize("family", ["tile", "ztile", "zwtile"])
+@pytest.mark.parametrize("family", ["tile", "wtile", "ztile", "zwtile"])
 def test_tiles_match_the_definitions(results, family):
     for (fam, typ, n), err in results.items():   # ztile n: 10 N + row blocks
         if fam != family:
