@@ -101,7 +101,8 @@ typedef struct quasi_config {
                            warp tiles per type; FFT or tensor-core x / y
                            passes in the BF16X3_TC form) on this grid and
                            keeps the fastest, remembered per grid and
-                           device for later handles; 0: fixed defaults    */
+                           device for later handles; 0: fixed defaults;
+                           2: every pass as warp tiles where it can be     */
 } quasi_config;
 
 typedef struct quasi_handle quasi_handle;

@@ -163,9 +163,12 @@ class Engine : public EngineBase {
     if (!layout_ok_) { err = "internal error: field layout does not match the slab sizes"; return QUASI_ERR_CUDA; }
     // the six step graphs are made here, like the reference's FFTW plans
     // before its loop: quasi_step only launches them
-    if (cfg_.autotune) {
+    if (cfg_.autotune == 1) {
       const int rc = autotune();
       if (rc) return rc;
+    } else if (cfg_.autotune == 2) {   // every warp-tile candidate (tests of those kernels)
+      tune_.zwarp[0] = tune_.zwarp[1] = true;
+      for (auto& a : tune_.xywarp) a[0] = a[1] = true;
     }
     return capture();
   }

@@ -233,3 +233,25 @@ def test_autotuner_choices_do_not_change_results():
     assert rel(out[0], out[1]) < 1e-6
     small = q.Simulation(q.default_config("stb", 16, 16, 32, precision="fp32"))   # no TMA z pass here
     assert small.tuning()["measured"]
+
+
+@pytest.mark.parametrize("grid", [(32, 32, 64), (64, 64, 128), (96, 96, 192)])
+def test_warp_tile_kernels_match_oracle(grid):
+    """Every pass as warp tiles (autotune = 2: the z, x and y kernels the
+    autotuner may pick) against the oracle, FP64, 3 steps."""
+    import smaiso_quasi_b200 as q
+    cfg = q.default_config("quasi", *grid, emulate_ranks=2, autotune=2)
+    m = qo.Model(nx=grid[0], ny=grid[1], nz=grid[2], emulate_ranks=2)
+    psi0 = qo.ic_field(m, "planar", seed=8)
+    sim = q.Simulation(cfg)
+    t = sim.tuning()
+    assert set(t["warp_tiles_double"]) == {"z", "x", "y"}
+    sim.set_psi(psi0)
+    sim.init()
+    o = qo.QuasiOracle(m)
+    o.set_psi(psi0)
+    o.init()
+    for _ in range(3):
+        o.step()
+    sim.step(3)
+    compare(sim, o, TOL64)
