@@ -527,7 +527,7 @@ class Engine : public EngineBase {
   }
   Header header() const {
     Header h{};
-    std::memcpy(h.magic, "QUASICK2", 8);
+    std::memcpy(h.magic, "QUASICK3", 8);
     h.nx = g_.nx; h.ny = g_.ny; h.nz = g_.nz; h.variant = cfg_.variant; h.elem = int(sizeof(T));
     h.nloop = nloop_;
     return h;
@@ -559,7 +559,8 @@ class Engine : public EngineBase {
     const size_t t = sizeof(T), d = sizeof(double);
     std::vector<Field> v = {{c_.psiq, d}, {c_.psiq_old, d}, {c_.Nq_old, t}, {c_.rhoq, d},  {c_.rho_old, d},
                             {c_.rho, d},  {c_.vx, t},       {c_.vy, t},     {c_.vz, t},    {c_.divv, t},
-                            {c_.divvq, t}, {c_.psi, d},     {c_.psi_old, d}, {c_.p, t},    {c_.df, t}};
+                            {c_.divvq, t}, {c_.psi, d},     {c_.psi_old, d}, {c_.p, t},    {c_.df, t},
+                            {c_.gx, d},    {c_.gy, d},      {c_.gz, d}};
     if constexpr (kStateCopy<T>) {
       v.push_back({c_.psiq_t, t});
       v.push_back({c_.rhoq_t, t});
@@ -742,7 +743,7 @@ class Engine : public EngineBase {
   int* nloop_dev_ = nullptr;
   double* partial_ = nullptr;
   cudaStream_t stream2_ = nullptr;
-  cudaEvent_t fork_ev_[8] = {};
+  cudaEvent_t fork_ev_[10] = {};
   int* tma_err_ = nullptr;
   int sms_ = 148;
   void* host_stage_ = nullptr;

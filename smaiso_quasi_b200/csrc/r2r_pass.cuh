@@ -907,6 +907,18 @@ struct ShiftKLoad {
   __device__ T operator()(int i, int j, int k) const { return k + 1 < g.nz ? src[lin(g, i, j, k + 1)] : T(0); }
 };
 
+// z loads shifted by one along k and scaled by -mk[k]: -mk[k] row[k + 1],
+// zero at the top (the general-kernel form of the z pass with ks = 2).
+template <typename T>
+struct ShiftKMulLoad {
+  Geom g;
+  const T* src;
+  const T* mk;
+  __device__ T operator()(int i, int j, int k) const {
+    return k + 1 < g.nz ? -mk[k] * src[lin(g, i, j, k + 1)] : T(0);
+  }
+};
+
 // Plain field loads: the persistent TMA kernel when the tile fits a box,
 // otherwise the general kernel above.  ks = 1 (z passes only) loads row[k + 1].
 template <typename T, int AXIS, class Store>
@@ -988,6 +1000,34 @@ cudaError_t launch_mul_x_pass(const Geom& g, int kind, Tables<T> tb, const T* sr
 #undef QUASI_TMA_CASE
   }
   return launch_pass<T, 0>(g, kind, tb, MulLoad<T, Mul>{g, src, mul, di, dj}, st, s);
+}
+
+// y pass whose input is mul(i,j,k) * src[i, j + 1, k] (the row past the end
+// reads as zero): the y pass of a y gradient taken after a plain x pass.
+template <typename T, class Mul, class Store>
+cudaError_t launch_mul_y_pass(const Geom& g, int kind, Tables<T> tb, const T* src, Mul mul, Store st, cudaStream_t s) {
+  const long extent = g.nz;
+  if (tma_config().enabled && tma_config().err) {
+#define QUASI_TMA_CASE(NN)                                                                            \
+    case NN: {                                                                                        \
+      constexpr int P = pass_pencils<T>(NN);                                                          \
+      if (extent % P == 0) return launch_tma_pass<T, NN, 1, P>(g, kind, tb, src, st, s, mul, 1, 0);   \
+      break;                                                                                          \
+    }
+    switch (g.ny) {
+      QUASI_TMA_CASE(16)
+      QUASI_TMA_CASE(32)
+      QUASI_TMA_CASE(64)
+      QUASI_TMA_CASE(96)
+      QUASI_TMA_CASE(128)
+      QUASI_TMA_CASE(192)
+      QUASI_TMA_CASE(256)
+      QUASI_TMA_CASE(512)
+      default: break;
+    }
+#undef QUASI_TMA_CASE
+  }
+  return launch_pass<T, 1>(g, kind, tb, MulLoad<T, Mul>{g, src, mul, 0, 1}, st, s);
 }
 
 // Two x passes of the same shifted source with different multipliers, one tile

@@ -663,9 +663,9 @@ constexpr int kiSTz[3] = {E01, E01, O01};
 
 static __global__ void bump_counter_kernel(int* n) { *n += 1; }
 
-#define QUASI_TRY(x)                          \
+#define QUASI_TRY(...)                        \
   do {                                        \
-    cudaError_t e_ = (x);                     \
+    cudaError_t e_ = (__VA_ARGS__);           \
     if (e_ != cudaSuccess) return e_;         \
   } while (0)
 
@@ -691,12 +691,63 @@ inline dim3 row_block(int nz) {
 #define QUASI_EW(kern, ...) kern<<<ew_grid(kern, 256), 256, 0, s>>>(__VA_ARGS__)
 #define QUASI_EW_ON(kern, strm, ...) kern<<<ew_grid(kern, 256), 256, 0, strm>>>(__VA_ARGS__)
 
+// z pass src -> dst: the TMA z kernel, else the general pass.  ks = 1
+// transforms row[k + 1] (zero at the top), ks = 2 -mk[k] row[k + 1].
+template <typename T>
+cudaError_t zpass(const Geom& g, int kind, Tables<T> tb, T* src, T* dst, cudaStream_t s, int ks = 0,
+                  const T* mk = nullptr) {
+  const cudaError_t e = launch_zpass<T>(g, kind, tb, src, dst, s, ks, mk);
+  if (e != cudaErrorNotSupported) return e;
+  if (ks == 2)
+    return launch_pass<T, 2, ShiftKMulLoad<T>, StoreField<T>>(g, kind, tb, ShiftKMulLoad<T>{g, src, mk},
+                                                              StoreField<T>{g, dst}, s);
+  return launch_pass<T, 2>(g, kind, tb, LoadField<T>{g, src}, StoreField<T>{g, dst}, s, ks);
+}
+
+// psi = iCT(psiq) (quasi.cpp:1963-1965) and grad psi (quasi.cpp:1120-1186) in
+// double, in 9 axis passes instead of 12.  Each transform is separable and
+// a multiplier or shift along one axis commutes with the passes along the
+// others, so psi, grad_y and grad_z share the plain x pass X of psiq, and psi
+// and grad_z share its plain y pass XY:
+//   s:  X = x(psiq);  grad_y = z(y'(X));  XY = y(X);  psi = z(XY);
+//       grad_z = z'(XY)
+//   s2: grad_x = z(y(x'(psiq)))
+// (a primed pass takes the shifted, scaled row and the odd kind: y' reads
+// -vs_y[j] X[j + 1], z' -vs_z[k] XY[k + 1], x' -vs_x[i] psiq[i + 1]).  ev: a
+// fork/join pair for the second stream (nullptr: everything on s).
+template <typename T>
+cudaError_t psi_and_grad(const StepCtx<T>& c, const AxisTables<double>& tb64, const double* psiq, double* psi,
+                         cudaStream_t s, cudaStream_t s2, const cudaEvent_t* ev) {
+  const Geom g = c.g;
+  const bool two = s2 && ev;
+  const cudaStream_t sb = two ? s2 : s;
+  if (two) {
+    QUASI_TRY(cudaEventRecord(ev[0], s));
+    QUASI_TRY(cudaStreamWaitEvent(s2, ev[0], 0));
+  }
+  QUASI_TRY(inverse3_mul(g, tb64, kiSTx, psiq, MGrad<T, 0, false>{c}, 1, 0, 0, StoreField<double>{g, c.gx}, c.gx,
+                         sb));
+  double* x = c.tmp64;
+  QUASI_TRY(launch_pass<double, 0>(g, E01, tb64.t[0], LoadField<double>{g, psiq}, StoreField<double>{g, x}, s));
+  QUASI_TRY(launch_mul_y_pass<double>(g, O01, tb64.t[1], x, MGrad<T, 1, false>{c}, StoreField<double>{g, c.gy}, s));
+  QUASI_TRY(zpass<double>(g, E01, tb64.t[2], c.gy, c.gy, s));
+  QUASI_TRY(launch_pass<double, 1>(g, E01, tb64.t[1], LoadField<double>{g, x}, StoreField<double>{g, x}, s));
+  QUASI_TRY(zpass<double>(g, E01, tb64.t[2], x, psi, s));
+  QUASI_TRY(zpass<double>(g, O01, tb64.t[2], x, c.gz, s, 2, c.vsz));
+  if (two) {
+    QUASI_TRY(cudaEventRecord(ev[1], s2));
+    QUASI_TRY(cudaStreamWaitEvent(s, ev[1], 0));
+  }
+  return cudaSuccess;
+}
+
 // One time step, enqueued on `s` (captured into a CUDA graph by the caller).
 // Independent transforms (the inverse transforms of psi^ and rho^, the three
 // stress transforms, the five after the projection) are split over s and a
 // second stream s2 between a fork and a join (ev[2i], ev[2i+1]; ev[6] orders
 // the second stream's stress transform after the stress kernel, ev[7] the
-// density chain after the gradients), so that in
+// density chain after the gradients, ev[8], ev[9] the fork and join of psi
+// and grad psi at the end), so that in
 // the captured graph one persistent pass kernel's last tiles overlap the next
 // one's first loads.  s2 == nullptr: everything on s.
 // tb64: the FP64 twiddles of the double transforms (the same tables as tb in
@@ -723,32 +774,18 @@ cudaError_t enqueue_step(const StepCtx<T>& c, const AxisTables<T>& tb, const Axi
   auto ld = [&](T* d) { return LoadField<T>{g, d}; };
   auto st64 = [&](double* d) { return StoreField<double>{g, d}; };
   if (c.variant == kQuasi) {
-    // a3 prologue quasi.cpp:1036-1057
-    // (pairs that share the source, kinds and shift take one dual x pass)
-    // a4 gradients quasi.cpp:1120-1232: grad psi with grad lap grad psi, grad rho
+    // a4 gradients quasi.cpp:1120-1232: grad lap grad psi from the transform
+    // copy of psi^, grad rho (grad psi in double is carried from the end of
+    // the previous step, where it shares passes with psi)
     QUASI_TRY(fork(0));
-    if constexpr (kStateCopy<T>) {
-      // grad psi in double from psi^ itself; grad lap grad psi in float from its copy
-      QUASI_TRY(inverse3_mul(g, tb64, kiSTx, c.psiq, MGrad<T, 0, false>{c}, 1, 0, 0, st64(c.gx), c.gx, s));
-      QUASI_TRY(inverse3_mul(g, tb, kiSTx, c.psiq_t, MGrad<T, 0, true>{c}, 1, 0, 0, st(c.ldx), c.ldx, sb));
-      QUASI_TRY(inverse3_mul(g, tb64, kiSTy, c.psiq, MGrad<T, 1, false>{c}, 0, 1, 0, st64(c.gy), c.gy, sb));
-      QUASI_TRY(inverse3_mul(g, tb, kiSTy, c.psiq_t, MGrad<T, 1, true>{c}, 0, 1, 0, st(c.ldy), c.ldy, s));
-      QUASI_TRY(inverse3_mul(g, tb64, kiSTz, c.psiq, MGrad<T, 2, false>{c}, 0, 0, 1, st64(c.gz), c.gz, s));
-      QUASI_TRY(inverse3_mul(g, tb, kiSTz, c.psiq_t, MGrad<T, 2, true>{c}, 0, 0, 1, st(c.ldz), c.ldz, sb));
-    } else {
-      // one dual x pass per axis: grad psi with grad lap grad psi
-      QUASI_TRY(inverse3_mul2(g, tb, kiSTx, c.psiq_t, MGrad<T, 0, false>{c}, MGrad<T, 0, true>{c}, 1, 0, 0,
-                              reinterpret_cast<T*>(c.gx), c.ldx, s));
-      QUASI_TRY(inverse3_mul2(g, tb, kiSTy, c.psiq_t, MGrad<T, 1, false>{c}, MGrad<T, 1, true>{c}, 0, 1, 0,
-                              reinterpret_cast<T*>(c.gy), c.ldy, sb));
-      QUASI_TRY(inverse3_mul2(g, tb, kiSTz, c.psiq_t, MGrad<T, 2, false>{c}, MGrad<T, 2, true>{c}, 0, 0, 1,
-                              reinterpret_cast<T*>(c.gz), c.ldz, s));
-    }
+    QUASI_TRY(inverse3_mul(g, tb, kiSTx, c.psiq_t, MGrad<T, 0, true>{c}, 1, 0, 0, st(c.ldx), c.ldx, s));
+    QUASI_TRY(inverse3_mul(g, tb, kiSTy, c.psiq_t, MGrad<T, 1, true>{c}, 0, 1, 0, st(c.ldy), c.ldy, sb));
+    QUASI_TRY(inverse3_mul(g, tb, kiSTz, c.psiq_t, MGrad<T, 2, true>{c}, 0, 0, 1, st(c.ldz), c.ldz, s));
     QUASI_TRY(inverse3_mul(g, tb, kiSTx, c.rhoq_t, MGrad<T, 0, false>{c}, 1, 0, 0, st(c.rdx), c.rdx, sb));
     QUASI_TRY(inverse3_mul(g, tb, kiSTy, c.rhoq_t, MGrad<T, 1, false>{c}, 0, 1, 0, st(c.rdy), c.rdy, s));
     QUASI_TRY(inverse3_mul(g, tb, kiSTz, c.rhoq_t, MGrad<T, 2, false>{c}, 0, 0, 1, st(c.rdz), c.rdz, sb));
-    // the density chain needs grad psi and must not rewrite rho^ before the grad
-    // rho transforms have read it: s waits for the second stream's share ...
+    // the density chain must not rewrite rho^ before the grad rho transforms
+    // have read it: s waits for the second stream's share ...
     if (s2) {
       QUASI_TRY(cudaEventRecord(ev[7], s2));
       QUASI_TRY(cudaStreamWaitEvent(s, ev[7], 0));
@@ -768,13 +805,9 @@ cudaError_t enqueue_step(const StepCtx<T>& c, const AxisTables<T>& tb, const Axi
     QUASI_TRY(join(0));
 
   } else {
-    // quasi-stb.cpp:1005-1038 (the unused dRho transform is elided)
-    QUASI_TRY(fork(0));
+    // quasi-stb.cpp:1005-1038 (the unused dRho transform is elided; grad psi
+    // is carried from the end of the previous step)
     QUASI_TRY(inverse3_mul(g, tb, kiCT, c.psiq_t, MSh<T>{c}, 0, 0, 0, st(c.sh), c.sh, s));
-    QUASI_TRY(inverse3_mul(g, tb64, kiSTx, c.psiq, MGrad<T, 0, false>{c}, 1, 0, 0, st64(c.gx), c.gx, sb));
-    QUASI_TRY(inverse3_mul(g, tb64, kiSTy, c.psiq, MGrad<T, 1, false>{c}, 0, 1, 0, st64(c.gy), c.gy, s));
-    QUASI_TRY(inverse3_mul(g, tb64, kiSTz, c.psiq, MGrad<T, 2, false>{c}, 0, 0, 1, st64(c.gz), c.gz, sb));
-    QUASI_TRY(join(0));
     // rho == 1, divv == 0, grad rho == 0 (rhoq never leaves 0): quasi-stb.cpp:1232
   }
   // a6 divv quasi.cpp:1273-1293 on the second stream, beside a7 the stress
@@ -827,8 +860,9 @@ cudaError_t enqueue_step(const StepCtx<T>& c, const AxisTables<T>& tb, const Axi
     update_kernel<T><<<per_sm * tma_config().sms, blk, 0, s>>>(c);
   }
   QUASI_TRY(cudaGetLastError());
-  // psi = iCT(psiq_new) in double; psi_old <- psi by rotation
-  QUASI_TRY(inverse3(g, tb64, kiCT, LoadField<double>{g, c.psiq_new}, c.tmp64, st64(c.psi_new), s));
+  // psi = iCT(psiq_new) and grad psi in double for the next step (psi_old <-
+  // psi by rotation)
+  QUASI_TRY(psi_and_grad(c, tb64, c.psiq_new, c.psi_new, s, s2, ev ? ev + 8 : nullptr));
   return cudaSuccess;
 }
 
@@ -881,7 +915,7 @@ cudaError_t enqueue_init(const StepCtx<T>& c, const AxisTables<T>& tb, const Axi
     to_storage_kernel<T><<<592, 256, 0, s>>>(c.psiq, c.psiq_t, n);
     QUASI_TRY(cudaGetLastError());
   }
-  QUASI_TRY(inverse3(g, tb64, kiCT, LoadField<double>{g, c.psiq}, c.psi, StoreField<double>{g, c.psi}, s));
+  QUASI_TRY(psi_and_grad(c, tb64, c.psiq, c.psi, s, nullptr, nullptr));
   QUASI_TRY(forward3(g, tb, kCT, LdInitN<T>{c}, c.Nq_old, StoreField<T>{g, c.Nq_old}, s));
   init_state_kernel<T><<<592, 256, 0, s>>>(c, n);
   QUASI_TRY(cudaGetLastError());

@@ -59,12 +59,15 @@ struct ZTile {
     int ks;
     QHD T at(int r, int n) const { return n + ks < N ? raw[ri(r, n + ks)] : T(0); }
   };
-  // the same with the shift fixed at compile time (the kernel's form)
+  // the same with the shift fixed at compile time (the kernel's form); KS = 2:
+  // row[n + 1] times -mk[n] (a z gradient's shift and wavenumber, zero at the top)
   template <int KS> struct RowsK {
     const T* raw;
+    const T* mk = nullptr;
     QHD T at(int r, int n) const {
       if constexpr (KS == 0) return raw[ri(r, n)];
-      else return n + KS < N ? raw[ri(r, n + KS)] : T(0);
+      else if constexpr (KS == 1) return n + 1 < N ? raw[ri(r, n + 1)] : T(0);
+      else return n + 1 < N ? -mk[n] * raw[ri(r, n + 1)] : T(0);
     }
   };
   template <class Src>
@@ -337,7 +340,7 @@ template <typename T> constexpr bool zpass_root_copy() { return sizeof(T) == 4; 
 template <typename T, int N, int P, int KS>
 __global__ void __launch_bounds__(256, 2)
     tma_zpass_kernel(const __grid_constant__ CUtensorMap src_map, const __grid_constant__ CUtensorMap dst_map, Geom g,
-                     int kind, Tables<T> tb, int ntiles, int* err, uint32_t polls, int skip) {
+                     int kind, Tables<T> tb, int ntiles, int* err, uint32_t polls, int skip, const T* mk) {
   constexpr int NT = 256, G = P / 2, SUB = (N + 255) / 256, BN = N / SUB;
   using Z = ZTile<T, N, G, NT, SUB>;
   constexpr bool kRootCopy = zpass_root_copy<T>();
@@ -400,7 +403,7 @@ __global__ void __launch_bounds__(256, 2)
     }
     // first stage: dense rows -> registers | previous store read out | -> padded tile
     typename Z::template Regs<Z::R1> r1;
-    Z::first_read(tid, typename Z::template RowsK<KS>{raw}, kind, tb, r1, tw1);
+    Z::first_read(tid, typename Z::template RowsK<KS>{raw, mk}, kind, tb, r1, tw1);
     if (tid == 0) bulk_wait_read0();
     __syncthreads();
     if (tid == 0 && t + 2 * int(gridDim.x) < ntiles && t + 2 * int(gridDim.x) != skip) {
@@ -452,7 +455,8 @@ struct ZwLayout {
 template <typename T, int N, int KS>
 __global__ void __launch_bounds__(256, 2)
     tma_zpass_warp_kernel(const __grid_constant__ CUtensorMap src_map, const __grid_constant__ CUtensorMap dst_map,
-                          Geom g, int kind, Tables<T> tb, int ntiles, int* err, uint32_t polls, int skip) {
+                          Geom g, int kind, Tables<T> tb, int ntiles, int* err, uint32_t polls, int skip,
+                          const T* mk) {
   using L = ZwLayout<T, N>;
   using Z = typename L::Z;
   constexpr int G = L::G, R = L::R, RAW = L::RAW;
@@ -513,7 +517,7 @@ __global__ void __launch_bounds__(256, 2)
       break;
     }
     typename Z::template Regs<Z::R1> r1;
-    Z::first_read(lane, typename Z::template RowsK<KS>{raw + b * RAW}, kind, tb, r1, tw1);
+    Z::first_read(lane, typename Z::template RowsK<KS>{raw + b * RAW, mk}, kind, tb, r1, tw1);
     if (lane == 0) bulk_wait_read0();   // the previous store has read the staging rows
     __syncwarp();
     const int tn = t + 2 * nwarps;
@@ -537,7 +541,8 @@ __global__ void __launch_bounds__(256, 2)
 }
 
 template <typename T, int N, int KS>
-cudaError_t launch_zpass_warp(const Geom& g, int kind, Tables<T> tb, const T* src, T* dst, cudaStream_t s) {
+cudaError_t launch_zpass_warp(const Geom& g, int kind, Tables<T> tb, const T* src, T* dst, cudaStream_t s,
+                              const T* mk) {
   using L = ZwLayout<T, N>;
   if (g.ny % L::R != 0) return cudaErrorNotSupported;
   const uint32_t box[3] = {uint32_t(N), uint32_t(L::R), 1};
@@ -560,7 +565,7 @@ cudaError_t launch_zpass_warp(const Geom& g, int kind, Tables<T> tb, const T* sr
   const int warps = per_sm * tma_config().sms * kZwWarps;
   const int grid = tiles < warps ? (tiles + kZwWarps - 1) / kZwWarps : per_sm * tma_config().sms;
   kern<<<grid, 256, smem, s>>>(smap, dmap, g, kind, tb, tiles, tma_config().err, tma_config().poll_limit,
-                               tma_config().skip_tile);
+                               tma_config().skip_tile, mk);
   return cudaGetLastError();
 }
 
@@ -569,7 +574,8 @@ cudaError_t launch_zpass_warp(const Geom& g, int kind, Tables<T> tb, const T* sr
 #endif
 
 template <typename T, int N, int KS>
-cudaError_t launch_zpass_nk(const Geom& g, int kind, Tables<T> tb, const T* src, T* dst, cudaStream_t s) {
+cudaError_t launch_zpass_nk(const Geom& g, int kind, Tables<T> tb, const T* src, T* dst, cudaStream_t s,
+                            const T* mk) {
   constexpr int P = pass_pencils<T>(N), G = P / 2, SUB = (N + 255) / 256;
   using Z = ZTile<T, N, G, 256, SUB>;
   if (g.ny % P != 0) return cudaErrorNotSupported;
@@ -593,37 +599,48 @@ cudaError_t launch_zpass_nk(const Geom& g, int kind, Tables<T> tb, const T* src,
   const int tiles = (g.nx * g.ny) / P;
   const int grid = tiles < per_sm * tma_config().sms ? tiles : per_sm * tma_config().sms;
   kern<<<grid, 256, smem, s>>>(smap, dmap, g, kind, tb, tiles, tma_config().err, tma_config().poll_limit,
-                               tma_config().skip_tile);
+                               tma_config().skip_tile, mk);
   return cudaGetLastError();
 }
 
+// ks: 0 plain, 1 row[k + 1], 2 row[k + 1] times -mk[k] (double passes only)
 template <typename T, int N>
-cudaError_t launch_zpass_n(const Geom& g, int kind, Tables<T> tb, const T* src, T* dst, cudaStream_t s, int ks) {
+cudaError_t launch_zpass_n(const Geom& g, int kind, Tables<T> tb, const T* src, T* dst, cudaStream_t s, int ks,
+                           const T* mk) {
+  if (ks == 2 && (sizeof(T) != 8 || !mk)) return cudaErrorNotSupported;
   if constexpr (N >= 64 && N <= 256) {
     if (tma_config().zwarp[sizeof(T) == 8]) {
-      const cudaError_t e = ks ? launch_zpass_warp<T, N, 1>(g, kind, tb, src, dst, s)
-                               : launch_zpass_warp<T, N, 0>(g, kind, tb, src, dst, s);
+      cudaError_t e;
+      if (ks == 0) e = launch_zpass_warp<T, N, 0>(g, kind, tb, src, dst, s, mk);
+      else if (ks == 1) e = launch_zpass_warp<T, N, 1>(g, kind, tb, src, dst, s, mk);
+      else if constexpr (sizeof(T) == 8) e = launch_zpass_warp<T, N, 2>(g, kind, tb, src, dst, s, mk);
+      else e = cudaErrorNotSupported;
       if (e != cudaErrorNotSupported) return e;
     }
   }
-  return ks ? launch_zpass_nk<T, N, 1>(g, kind, tb, src, dst, s) : launch_zpass_nk<T, N, 0>(g, kind, tb, src, dst, s);
+  if (ks == 0) return launch_zpass_nk<T, N, 0>(g, kind, tb, src, dst, s, mk);
+  if (ks == 1) return launch_zpass_nk<T, N, 1>(g, kind, tb, src, dst, s, mk);
+  if constexpr (sizeof(T) == 8) return launch_zpass_nk<T, N, 2>(g, kind, tb, src, dst, s, mk);
+  return cudaErrorNotSupported;
 }
 
 // z pass src -> dst (plain fields; ks = 1 transforms row[k + 1], zero at the
-// top) on the TMA load/store kernel; cudaErrorNotSupported when the shape or
-// configuration does not allow it (the caller takes the general pass).
+// top; ks = 2 also multiplies it by -mk[k]) on the TMA load/store kernel;
+// cudaErrorNotSupported when the shape or configuration does not allow it
+// (the caller takes the general pass).
 template <typename T>
-cudaError_t launch_zpass(const Geom& g, int kind, Tables<T> tb, const T* src, T* dst, cudaStream_t s, int ks = 0) {
+cudaError_t launch_zpass(const Geom& g, int kind, Tables<T> tb, const T* src, T* dst, cudaStream_t s, int ks = 0,
+                         const T* mk = nullptr) {
   if (!QUASI_ZPASS || !tma_config().enabled || !tma_config().err) return cudaErrorNotSupported;
   switch (g.nz) {
-    case 16: return launch_zpass_n<T, 16>(g, kind, tb, src, dst, s, ks);
-    case 32: return launch_zpass_n<T, 32>(g, kind, tb, src, dst, s, ks);
-    case 64: return launch_zpass_n<T, 64>(g, kind, tb, src, dst, s, ks);
-    case 96: return launch_zpass_n<T, 96>(g, kind, tb, src, dst, s, ks);
-    case 128: return launch_zpass_n<T, 128>(g, kind, tb, src, dst, s, ks);
-    case 192: return launch_zpass_n<T, 192>(g, kind, tb, src, dst, s, ks);
-    case 256: return launch_zpass_n<T, 256>(g, kind, tb, src, dst, s, ks);
-    case 512: return launch_zpass_n<T, 512>(g, kind, tb, src, dst, s, ks);
+    case 16: return launch_zpass_n<T, 16>(g, kind, tb, src, dst, s, ks, mk);
+    case 32: return launch_zpass_n<T, 32>(g, kind, tb, src, dst, s, ks, mk);
+    case 64: return launch_zpass_n<T, 64>(g, kind, tb, src, dst, s, ks, mk);
+    case 96: return launch_zpass_n<T, 96>(g, kind, tb, src, dst, s, ks, mk);
+    case 128: return launch_zpass_n<T, 128>(g, kind, tb, src, dst, s, ks, mk);
+    case 192: return launch_zpass_n<T, 192>(g, kind, tb, src, dst, s, ks, mk);
+    case 256: return launch_zpass_n<T, 256>(g, kind, tb, src, dst, s, ks, mk);
+    case 512: return launch_zpass_n<T, 512>(g, kind, tb, src, dst, s, ks, mk);
     default: return cudaErrorNotSupported;
   }
 }
