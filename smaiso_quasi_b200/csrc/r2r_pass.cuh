@@ -310,26 +310,49 @@ struct RowStageValSnk {
 // Identity multiplier (plain passes).
 struct NoMul {
   static constexpr bool kActive = false;
+  template <int AX> static constexpr bool kTable = false;
   __device__ double operator()(int, int, int) const { return 1.0; }
 };
+
+// Axis tables.  A multiplier whose dependence on the index n along a pass's
+// axis AX goes through one double wavenumber table sets kTable<AX> and gives
+//   const double* axis_table(int ax)         the table (N entries)
+//   Col col_at(int ax, int outer, int k)      the rest, once per pencil
+//   double from(int ax, double w, const Col&)  the multiplier, w = table[n]
+// The x / y kernels copy the table into shared memory once per CTA (when two
+// CTAs per SM still fit), so the per-element work reads shared memory only.
+template <class M, int AX> constexpr bool axis_tab() { return M::kActive && M::template kTable<AX>; }
+
+// Tables a pass kernel stages: one per multiplier, 0 unless every active
+// multiplier has one on this axis and the kernel still fits twice per SM.
+template <int AX, class Mul, class Mul2>
+constexpr int row_tables(size_t base_smem, int n) {
+  constexpr bool dual = Mul2::kActive;
+  constexpr int want = axis_tab<Mul, AX>() && (!dual || axis_tab<Mul2, AX>()) ? (dual ? 2 : 1) : 0;
+  return want && 2 * (base_smem + size_t(want) * n * sizeof(double) + 1024) <= 233472 ? want : 0;
+}
 
 template <class M, class = void> struct MulCol { struct type {}; };
 template <class M> struct MulCol<M, std::void_t<typename M::Col>> { using type = typename M::Col; };
 
 // x / y tile source with a per-element multiplier of the OUTPUT index
 // (i, j, k): the spectral prologue of an inverse transform.
-template <typename T, int AXIS, class Mul, bool ALIAS = false>
+template <typename T, int AXIS, class Mul, bool ALIAS = false, bool TAB = false>
 struct MulSrc {
   static constexpr bool kAliasesTile = ALIAS;
   const T* raw;
   int P, outer, k0;
   Mul mul;
-  // x passes: the column parts of this thread's two pencils (prep)
+  // x passes (and TAB): the column parts of this thread's two pencils (prep)
   typename MulCol<Mul>::type ca{}, cb{};
+  const double* tab = nullptr;   // TAB: the multiplier's axis table in shared memory
   // gt = the one pencil pair this thread reads: the first stage's pencil-fastest
   // mapping gives g = tid % (P/2) whenever the thread count is a multiple of P/2
   __device__ void prep(int gt) {
-    if constexpr (Mul::kActive && AXIS == 0) {
+    if constexpr (TAB) {
+      ca = mul.col_at(AXIS, outer, k0 + 2 * gt);
+      cb = mul.col_at(AXIS, outer, k0 + 2 * gt + 1);
+    } else if constexpr (Mul::kActive && AXIS == 0) {
       ca = mul.col(outer, k0 + 2 * gt);
       cb = mul.col(outer, k0 + 2 * gt + 1);
     }
@@ -341,7 +364,11 @@ struct MulSrc {
     if constexpr (Mul::kActive) {
       // the multiplier is evaluated in its own type (double where q0^2 - q^2
       // cancels), rounded to the storage type once, and applied there
-      if constexpr (AXIS == 0) {
+      if constexpr (TAB) {
+        const double w = tab[n];
+        a *= T(mul.from(AXIS, w, ca));
+        b *= T(mul.from(AXIS, w, cb));
+      } else if constexpr (AXIS == 0) {
         a *= T(mul.row(n, ca));
         b *= T(mul.row(n, cb));
       } else {
@@ -410,7 +437,8 @@ template <typename T, int N, int P> constexpr int tma_work_elems() { return ((P 
 // over the work tile and one thread stores the tile through dmap (dmap2 for
 // the dual pass's second output); the next tile's first stage waits for the
 // store to have read them.
-template <typename T, int N, int AXIS, int P, class Store, class Mul, class Mul2 = NoMul, bool TSTORE = false>
+template <typename T, int N, int AXIS, int P, class Store, class Mul, class Mul2 = NoMul, bool TSTORE = false,
+          int TABS = 0>
 __global__ void __launch_bounds__(tma_threads<T>(), 2)
     tma_pass_kernel(const __grid_constant__ CUtensorMap map, Geom g, int kind, Tables<T> tb, Store st, int ntiles,
                     int* err, uint32_t polls, int skip, Mul mul, int dc1, int dc2, int ks, Store st2, Mul2 mul2,
@@ -427,14 +455,18 @@ __global__ void __launch_bounds__(tma_threads<T>(), 2)
   T* raw1 = raw0 + P * N;
   T* work = raw1 + P * N;
   uint64_t* bar = reinterpret_cast<uint64_t*>(work + tma_work_elems<T, N, P>());
+  double* atab = reinterpret_cast<double*>(reinterpret_cast<Cx<T>*>(bar + 2) + 2 * N);
   const int tid = threadIdx.x;
   {
     // per-CTA shared-memory copies of the twiddle tables (N entries each)
+    // and of the multipliers' axis tables (TABS of N doubles)
     Cx<T>* rt = reinterpret_cast<Cx<T>*>(bar + 2);
     Cx<T>* qt = rt + N;
     for (int e = tid; e < N; e += NT) {
       rt[e] = tb.root[e];
       qt[e] = tb.quarter[e];
+      if constexpr (TABS > 0) atab[e] = mul.axis_table(AXIS)[e];
+      if constexpr (TABS > 1) atab[N + e] = mul2.axis_table(AXIS)[e];
     }
     tb.root = rt;
     tb.quarter = qt;
@@ -496,7 +528,8 @@ __global__ void __launch_bounds__(tma_threads<T>(), 2)
     if constexpr (AXIS != 2 && kDual) {
       const int kt = g.nz / P;
       const int outer = t / kt, k0 = (t - outer * kt) * P;
-      MulSrc<T, AXIS, Mul> src{raw, P, outer, k0, mul};
+      MulSrc<T, AXIS, Mul, false, (TABS > 0)> src{raw, P, outer, k0, mul};
+      src.tab = atab;
       src.prep(tid % (P / 2));
       if constexpr (TSTORE) {
         r2r_tile<T, N, P / 2, NT, false>(ex, tid, kind, reinterpret_cast<Cx<T>*>(work), src,
@@ -508,7 +541,8 @@ __global__ void __launch_bounds__(tma_threads<T>(), 2)
                                           GlobSnk<T, AXIS, Store>{st, outer, k0}, tb);
       }
       __syncthreads();   // the second transform rewrites the work tile
-      MulSrc<T, AXIS, Mul2> src2{raw, P, outer, k0, mul2};
+      MulSrc<T, AXIS, Mul2, false, (TABS > 1)> src2{raw, P, outer, k0, mul2};
+      src2.tab = atab + N;
       src2.prep(tid % (P / 2));
       if constexpr (TSTORE) {
         r2r_tile<T, N, P / 2, NT, false>(ex, tid, kind, reinterpret_cast<Cx<T>*>(work), src2,
@@ -521,7 +555,8 @@ __global__ void __launch_bounds__(tma_threads<T>(), 2)
     } else if constexpr (AXIS != 2) {
       const int kt = g.nz / P;
       const int outer = t / kt, k0 = (t - outer * kt) * P;
-      MulSrc<T, AXIS, Mul> src{raw, P, outer, k0, mul};
+      MulSrc<T, AXIS, Mul, false, (TABS > 0)> src{raw, P, outer, k0, mul};
+      src.tab = atab;
       src.prep(tid % (P / 2));
       if constexpr (TSTORE && IsStoreField<Store>::value) {
         r2r_tile<T, N, P / 2, NT, false>(ex, tid, kind, reinterpret_cast<Cx<T>*>(work), src,
@@ -604,7 +639,8 @@ struct XywLayout {
   static_assert(RAW <= WORK, "the staging rows overlay the work tile");
 };
 
-template <typename T, int N, int AXIS, class Store, class Mul, class Mul2 = NoMul, bool TSTORE = false>
+template <typename T, int N, int AXIS, class Store, class Mul, class Mul2 = NoMul, bool TSTORE = false,
+          int TABS = 0>
 __global__ void __launch_bounds__(256, 2)
     tma_pass_warp_kernel(const __grid_constant__ CUtensorMap map, Geom g, int kind, Tables<T> tb, Store st,
                          int ntiles, int* err, uint32_t polls, int skip, Mul mul, int dc1, int dc2, Store st2,
@@ -622,12 +658,15 @@ __global__ void __launch_bounds__(256, 2)
   T* work = raw1 + RAW;
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + size_t(kXywWarps) * L::per_warp());
   uint64_t* bar = bars + 2 * warp;
+  double* atab = reinterpret_cast<double*>(reinterpret_cast<Cx<T>*>(bars + 2 * kXywWarps) + 2 * N);
   {
     Cx<T>* rt = reinterpret_cast<Cx<T>*>(bars + 2 * kXywWarps);
     Cx<T>* qt = rt + N;
     for (int e = tid; e < N; e += 256) {
       rt[e] = tb.root[e];
       qt[e] = tb.quarter[e];
+      if constexpr (TABS > 0) atab[e] = mul.axis_table(AXIS)[e];
+      if constexpr (TABS > 1) atab[N + e] = mul2.axis_table(AXIS)[e];
     }
     tb.root = rt;
     tb.quarter = qt;
@@ -677,7 +716,8 @@ __global__ void __launch_bounds__(256, 2)
     };
     const int kt = g.nz / PW;
     const int outer = t / kt, k0 = (t - outer * kt) * PW;
-    MulSrc<T, AXIS, Mul> src{raw, PW, outer, k0, mul};
+    MulSrc<T, AXIS, Mul, false, (TABS > 0)> src{raw, PW, outer, k0, mul};
+    src.tab = atab;
     src.prep(lane % G);
     if constexpr (kDual) {
       if constexpr (TSTORE) {
@@ -689,7 +729,8 @@ __global__ void __launch_bounds__(256, 2)
                                      GlobSnk<T, AXIS, Store>{st, outer, k0}, tb);
       }
       __syncwarp();   // the second transform rewrites the work tile
-      MulSrc<T, AXIS, Mul2> src2{raw, PW, outer, k0, mul2};
+      MulSrc<T, AXIS, Mul2, false, (TABS > 1)> src2{raw, PW, outer, k0, mul2};
+      src2.tab = atab + N;
       src2.prep(lane % G);
       if constexpr (TSTORE) {
         r2r_tile<T, N, G, 32, false>(ex, lane, kind, reinterpret_cast<Cx<T>*>(work), src2, RowStageSnk<T>{work, PW}, tb,
@@ -719,7 +760,7 @@ __global__ void __launch_bounds__(256, 2)
 }
 
 template <typename T, int N, int P>
-inline size_t tma_smem_bytes() {
+constexpr size_t tma_smem_bytes() {
   return size_t(2) * P * N * sizeof(T) + size_t(tma_work_elems<T, N, P>()) * sizeof(T) + 16 +
          2 * N * sizeof(Cx<T>);
 }
@@ -765,6 +806,10 @@ struct TmaConfig {
   // x [0] / y [1] passes as warp tiles (tma_pass_warp_kernel), float / double
   bool xywarp[2][2] = {{false, false}, {false, false}};
   int tc_axes = 3;        // with tc: the axes (bit 0 x, bit 1 y) that use it
+  // z passes walk their tiles from the last x plane to the first, so that they
+  // start on the rows the pass before them (a y pass or an elementwise stage,
+  // both first plane to last) wrote last, which are still in L2
+  bool zrev = false;
   int sms = 148;          // CTAs per SM x SMs bounds the persistent grid
   bool enabled = true;
 };
@@ -799,8 +844,9 @@ cudaError_t launch_tma_pass_warp(const Geom& g, int kind, Tables<T> tb, const T*
         return cudaErrorNotSupported;
     }
   }
-  const size_t smem = L::smem_bytes();
-  auto kern = tma_pass_warp_kernel<T, N, AXIS, Store, Mul, Mul2, TSTORE>;
+  constexpr int TABS = row_tables<AXIS, Mul, Mul2>(L::smem_bytes(), N);
+  const size_t smem = L::smem_bytes() + size_t(TABS) * N * sizeof(double);
+  auto kern = tma_pass_warp_kernel<T, N, AXIS, Store, Mul, Mul2, TSTORE, TABS>;
   static int per_sm = 0;   // per instantiation: resident CTAs per SM
   if (per_sm == 0) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -850,8 +896,9 @@ cudaError_t launch_tma_pass(const Geom& g, int kind, Tables<T> tb, const T* src,
         return cudaErrorNotSupported;
     }
   }
-  const size_t smem = tma_smem_bytes<T, N, P>();
-  auto kern = tma_pass_kernel<T, N, AXIS, P, Store, Mul, Mul2, TSTORE>;
+  constexpr int TABS = AXIS == 2 ? 0 : row_tables<AXIS, Mul, Mul2>(tma_smem_bytes<T, N, P>(), N);
+  const size_t smem = tma_smem_bytes<T, N, P>() + size_t(TABS) * N * sizeof(double);
+  auto kern = tma_pass_kernel<T, N, AXIS, P, Store, Mul, Mul2, TSTORE, TABS>;
   static int per_sm = 0;   // per instantiation: resident CTAs per SM
   if (per_sm == 0) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -1,9 +1,12 @@
 // The quasi-incompressible smectic-isotropic time step (quasi.cpp:1014-1965)
-// and its stability variant (quasi-stb.cpp:983-1968) as a sequence of fused
-// axis passes.  Every pointwise triple loop of the reference becomes the
-// loader (first pass) or storer (last pass) of the transform that consumes or
-// produces it, so no intermediate array of the reference is materialised
-// unless a later stage reads it.
+// and its stability variant (quasi-stb.cpp:983-1968) as a sequence of axis
+// passes and elementwise stages.  The spectral multipliers and index shifts
+// of the reference's pointwise loops (df, lap, -aLin, the shifted gradients,
+// the density filter, the scale factors) are applied by the loader of the
+// first pass or the storer of the last pass of the transform they belong to;
+// the stages that combine several real-space fields (density law, divv,
+// stress, projection, nonlinear term, update) are one elementwise kernel
+// each, reading every input once in 16-byte packs.
 //
 // Templated on the storage/transform type T (double: the plain FP64 form;
 // float: the FP32 form).  Wavenumbers, spectral constants, the semi-implicit
@@ -84,50 +87,65 @@ __device__ __forceinline__ double mq2c(const StepCtx<T>& c, int i, int j, int k)
 // Each multiplier splits into a column part (j, k: fixed for a thread of an
 // x-pass tile, computed once per tile) and a row part (i, per element):
 // row(i, col(j, k)) == operator()(i, j, k).
+// On x passes the row part reads one wavenumber table (the axis-table
+// protocol of the pass kernels: from(0, w, cl) == row(i, cl) for w = table[i]).
 template <typename T> struct MDf {      // dfDlapPsi, quasi.cpp:1044
   static constexpr bool kActive = true;
+  template <int AX> static constexpr bool kTable = AX == 0;
   StepCtx<T> c;
   struct Col { double s; };             // qy^2 + qz^2
   __device__ Col col(int j, int k) const {
     const double y = __ldg(c.vqy + j), z = __ldg(c.vqz + k);
     return {y * y + z * z};
   }
-  __device__ double q2(int i, const Col& cl) const {   // quasi.cpp:882
-    const double x = __ldg(c.vqx + i);
-    return x * x + cl.s;
-  }
-  __device__ double row(int i, const Col& cl) const { return c.alpha * (c.q0 * c.q0 - q2(i, cl)); }
+  __device__ static double q2w(double x, const Col& cl) { return x * x + cl.s; }   // quasi.cpp:882
+  __device__ double q2(int i, const Col& cl) const { return q2w(__ldg(c.vqx + i), cl); }
+  __device__ double from(int, double x, const Col& cl) const { return c.alpha * (c.q0 * c.q0 - q2w(x, cl)); }
+  __device__ double row(int i, const Col& cl) const { return from(0, __ldg(c.vqx + i), cl); }
   __device__ double operator()(int i, int j, int k) const { return row(i, col(j, k)); }
+  __device__ const double* axis_table(int) const { return c.vqx; }
+  __device__ Col col_at(int, int j, int k) const { return col(j, k); }
 };
 template <typename T> struct MLap {     // lapRhoDfDlapPsi, quasi.cpp:1046-1047
   static constexpr bool kActive = true;
+  template <int AX> static constexpr bool kTable = AX == 0;
   StepCtx<T> c;
   using Col = typename MDf<T>::Col;
   __device__ Col col(int j, int k) const { return MDf<T>{c}.col(j, k); }
-  __device__ double row(int i, const Col& cl) const {
-    const double q2 = MDf<T>{c}.q2(i, cl);
+  __device__ double from(int, double x, const Col& cl) const {
+    const double q2 = MDf<T>::q2w(x, cl);
     return -q2 * (c.alpha * (c.q0 * c.q0 - q2));
   }
+  __device__ double row(int i, const Col& cl) const { return from(0, __ldg(c.vqx + i), cl); }
   __device__ double operator()(int i, int j, int k) const { return row(i, col(j, k)); }
+  __device__ const double* axis_table(int) const { return c.vqx; }
+  __device__ Col col_at(int, int j, int k) const { return col(j, k); }
 };
 template <typename T> struct MSh {      // -aLin, quasi-stb.cpp:1019
   static constexpr bool kActive = true;
+  template <int AX> static constexpr bool kTable = AX == 0;
   StepCtx<T> c;
   using Col = typename MDf<T>::Col;
   __device__ Col col(int j, int k) const { return MDf<T>{c}.col(j, k); }
-  __device__ double row(int i, const Col& cl) const {
-    const double d = c.q0 * c.q0 - MDf<T>{c}.q2(i, cl);
+  __device__ double from(int, double x, const Col& cl) const {
+    const double d = c.q0 * c.q0 - MDf<T>::q2w(x, cl);
     return -(c.ep - c.alpha * (d * d));
   }
+  __device__ double row(int i, const Col& cl) const { return from(0, __ldg(c.vqx + i), cl); }
   __device__ double operator()(int i, int j, int k) const { return row(i, col(j, k)); }
+  __device__ const double* axis_table(int) const { return c.vqx; }
+  __device__ Col col_at(int, int j, int k) const { return col(j, k); }
 };
 // Shifted gradient along A, quasi.cpp:1120-1186.  The input is read at
 // index + 1 along x or y by the TMA box offset (the row past the end reads as
 // zero: the reference's zero top DST index); along z the z pass shifts each
 // row by one when it stages it, so the multiplier here uses k - 1.
-// -vs_A, or with LAP |q_s|^2 vs_A (the shifted wavenumber on axis A).
+// -vs_A, or with LAP |q_s|^2 vs_A (the shifted wavenumber on axis A).  Axis
+// tables: on x passes the x wavenumber (where the row part depends on i); on
+// y passes -vs_y alone (the y gradient's multiplier after a plain x pass).
 template <typename T, int A, bool LAP> struct MGrad {
   static constexpr bool kActive = true;
+  template <int AX> static constexpr bool kTable = (AX == 0 && (A == 0 || LAP)) || (AX == 1 && A == 1 && !LAP);
   StepCtx<T> c;
   struct Col { double vs, s; bool zero; };   // vs_A (A = 1, 2); the j, k part of |q_s|^2
   __device__ Col col(int j, int k) const {
@@ -140,13 +158,21 @@ template <typename T, int A, bool LAP> struct MGrad {
     cl.s = y * y + z * z;
     return cl;
   }
-  __device__ double row(int i, const Col& cl) const {
+  // x = the x wavenumber of row i (vs_x for A = 0, else vq_x); on y passes
+  // (AX = 1) x = vs_y[j]
+  __device__ double from(int ax, double x, const Col& cl) const {
+    if (ax == 1) return -x;
     if (A == 2 && cl.zero) return 0.0;
-    if (!LAP) return A == 0 ? -__ldg(c.vsx + i) : -cl.vs;
-    const double x = A == 0 ? __ldg(c.vsx + i) : __ldg(c.vqx + i);
+    if (!LAP) return A == 0 ? -x : -cl.vs;
     return (x * x + cl.s) * (A == 0 ? x : cl.vs);   // -mq * (-vs)
   }
+  __device__ double row(int i, const Col& cl) const {
+    if (!LAP && A != 0) return from(0, 0.0, cl);
+    return from(0, __ldg((A == 0 ? c.vsx : c.vqx) + i), cl);
+  }
   __device__ double operator()(int i, int j, int k) const { return row(i, col(j, k)); }
+  __device__ const double* axis_table(int ax) const { return ax == 1 ? c.vsy : (A == 0 ? c.vsx : c.vqx); }
+  __device__ Col col_at(int ax, int outer, int k) const { return ax == 1 ? Col{0.0, 0.0, false} : col(outer, k); }
 };
 
 // ---------------------------------------------------------------------------

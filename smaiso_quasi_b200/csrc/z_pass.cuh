@@ -340,7 +340,7 @@ template <typename T> constexpr bool zpass_root_copy() { return sizeof(T) == 4; 
 template <typename T, int N, int P, int KS>
 __global__ void __launch_bounds__(256, 2)
     tma_zpass_kernel(const __grid_constant__ CUtensorMap src_map, const __grid_constant__ CUtensorMap dst_map, Geom g,
-                     int kind, Tables<T> tb, int ntiles, int* err, uint32_t polls, int skip, const T* mk) {
+                     int kind, Tables<T> tb, int ntiles, int* err, uint32_t polls, int skip, const T* mk, int rev) {
   constexpr int NT = 256, G = P / 2, SUB = (N + 255) / 256, BN = N / SUB;
   using Z = ZTile<T, N, G, NT, SUB>;
   constexpr bool kRootCopy = zpass_root_copy<T>();
@@ -368,7 +368,7 @@ __global__ void __launch_bounds__(256, 2)
     if constexpr (kRootCopy) tb.root = rt;
   }
   auto origin = [&](int t, int& c1, int& c2) {
-    const int row = t * P;
+    const int row = (rev ? ntiles - 1 - t : t) * P;
     c2 = row / g.ny;
     c1 = row - c2 * g.ny;
   };
@@ -456,7 +456,7 @@ template <typename T, int N, int KS>
 __global__ void __launch_bounds__(256, 2)
     tma_zpass_warp_kernel(const __grid_constant__ CUtensorMap src_map, const __grid_constant__ CUtensorMap dst_map,
                           Geom g, int kind, Tables<T> tb, int ntiles, int* err, uint32_t polls, int skip,
-                          const T* mk) {
+                          const T* mk, int rev) {
   using L = ZwLayout<T, N>;
   using Z = typename L::Z;
   constexpr int G = L::G, R = L::R, RAW = L::RAW;
@@ -491,7 +491,7 @@ __global__ void __launch_bounds__(256, 2)
   __syncthreads();   // tables and barriers ready: the only CTA-wide barrier
   const int w0 = int(blockIdx.x) * kZwWarps + warp, nwarps = int(gridDim.x) * kZwWarps;
   auto origin = [&](int t, int& c1, int& c2) {
-    const int row = t * R;   // R rows of one x plane (R divides ny)
+    const int row = (rev ? ntiles - 1 - t : t) * R;   // R rows of one x plane (R divides ny)
     c2 = row / g.ny;
     c1 = row - c2 * g.ny;
   };
@@ -565,7 +565,7 @@ cudaError_t launch_zpass_warp(const Geom& g, int kind, Tables<T> tb, const T* sr
   const int warps = per_sm * tma_config().sms * kZwWarps;
   const int grid = tiles < warps ? (tiles + kZwWarps - 1) / kZwWarps : per_sm * tma_config().sms;
   kern<<<grid, 256, smem, s>>>(smap, dmap, g, kind, tb, tiles, tma_config().err, tma_config().poll_limit,
-                               tma_config().skip_tile, mk);
+                               tma_config().skip_tile, mk, int(tma_config().zrev));
   return cudaGetLastError();
 }
 
@@ -599,7 +599,7 @@ cudaError_t launch_zpass_nk(const Geom& g, int kind, Tables<T> tb, const T* src,
   const int tiles = (g.nx * g.ny) / P;
   const int grid = tiles < per_sm * tma_config().sms ? tiles : per_sm * tma_config().sms;
   kern<<<grid, 256, smem, s>>>(smap, dmap, g, kind, tb, tiles, tma_config().err, tma_config().poll_limit,
-                               tma_config().skip_tile, mk);
+                               tma_config().skip_tile, mk, int(tma_config().zrev));
   return cudaGetLastError();
 }
 
