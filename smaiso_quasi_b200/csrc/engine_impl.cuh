@@ -2,7 +2,6 @@
 // and engine_f32.cu, which instantiate it for double and float.
 #pragma once
 #include <cstdint>
-#include <cstdlib>
 #include <fstream>
 #include <mutex>
 
@@ -605,7 +604,6 @@ class Engine : public EngineBase {
     t.tc_axes = tune_.tc_axes;
     t.zwarp[0] = tune_.zwarp[0];
     t.zwarp[1] = tune_.zwarp[1];
-    t.zrev = tune_.zrev;
     for (int a = 0; a < 2; ++a)
       for (int d = 0; d < 2; ++d) t.xywarp[a][d] = tune_.xywarp[a][d];
   }
@@ -739,7 +737,6 @@ class Engine : public EngineBase {
     bool xywarp[2][2] = {{false, false}, {false, false}};   // [axis x, y][float, double]
     int tc_axes = 3;
     bool measured = false;
-    bool zrev = std::getenv("QUASI_ZREV") && std::getenv("QUASI_ZREV")[0] == '1';
   } tune_;
   bool layout_ok_ = false;
   double* tabs_ = nullptr;

@@ -39,6 +39,21 @@ template <typename T> QHD Cx<T> cscale(Cx<T> a, T s) { return {a.x * s, a.y * s}
 template <typename T> QHD Cx<T> conj(Cx<T> a) { return {a.x, -a.y}; }
 template <typename T> QHD Cx<T> mul_mi(Cx<T> a) { return {a.y, -a.x}; }   // -i * a
 
+// FP32 complex adds and scales on sm_100's packed FP32x2 instructions (one
+// FADD2 / FMUL2 per complex add or scale; each lane rounds as the scalar
+// instruction does, so results are unchanged).  Complex products stay scalar:
+// packing their operands ((a.x, a.x), (b.y, b.x), ...) costs register moves
+// that outweigh the saving.
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+__device__ __forceinline__ float2 f2(Cx<float> a) { return make_float2(a.x, a.y); }
+__device__ __forceinline__ Cx<float> cf(float2 a) { return Cx<float>{a.x, a.y}; }
+__device__ __forceinline__ Cx<float> operator+(Cx<float> a, Cx<float> b) { return cf(__fadd2_rn(f2(a), f2(b))); }
+__device__ __forceinline__ Cx<float> operator-(Cx<float> a, Cx<float> b) {
+  return cf(__fadd2_rn(f2(a), make_float2(-b.x, -b.y)));
+}
+__device__ __forceinline__ Cx<float> cscale(Cx<float> a, float s) { return cf(__fmul2_rn(f2(a), make_float2(s, s))); }
+#endif
+
 enum Kind : int { E10 = 0, E01 = 1, O10 = 2, O01 = 3 };
 QHD bool is_forward(int kind) { return kind == E10 || kind == O10; }
 QHD bool is_sine(int kind) { return kind == O10 || kind == O01; }

@@ -809,7 +809,7 @@ struct TmaConfig {
   // z passes walk their tiles from the last x plane to the first, so that they
   // start on the rows the pass before them (a y pass or an elementwise stage,
   // both first plane to last) wrote last, which are still in L2
-  bool zrev = false;
+  bool zrev = true;
   int sms = 148;          // CTAs per SM x SMs bounds the persistent grid
   bool enabled = true;
 };
