@@ -64,7 +64,8 @@ class Engine : public EngineBase {
   // fields of the storage type (+ the float copies of psiq and rhoq); then
   // the double fields: psiq x 3, rhoq, rho, rho_old, psi x 2, grad psi x 3
   // (+ the scratch of the double transforms in the FP32 form)
-  static constexpr int kFields = 22 + (kStateCopy<T> ? 2 : 0);
+  // FP32: + the float copies of psi^, rho^; FP64: + the second grad rho buffers
+  static constexpr int kFields = 22 + (kStateCopy<T> ? 2 : 3);
   static constexpr int kDFields = 11 + (kStateCopy<T> ? 1 : 0);
   static constexpr int kPhases = 6;   // lcm of the 3-buffer psiq and 2-buffer Nq rotations
 
@@ -564,6 +565,10 @@ class Engine : public EngineBase {
     if constexpr (kStateCopy<T>) {
       v.push_back({c_.psiq_t, t});
       v.push_back({c_.rhoq_t, t});
+    } else {   // grad rho, computed by the previous step
+      v.push_back({c_.rdx, t});
+      v.push_back({c_.rdy, t});
+      v.push_back({c_.rdz, t});
     }
     return v;
   }
@@ -579,7 +584,8 @@ class Engine : public EngineBase {
   // psiq = A[s%3], psiq_old = A[(s+2)%3], psiq_new = A[(s+1)%3];
   // Nq (computed this step) = B[s%2], Nq_old = B[(s+1)%2];
   // psi = C[s%2], psi_old = psi_new = C[(s+1)%2] (psi_old is read only by the
-  // diagnostics after the step, when it is C[s%2] again).
+  // diagnostics after the step, when it is C[s%2] again);
+  // FP64 form: grad rho read = R[s%2], grad rho for the next step = R[(s+1)%2].
   void set_phase(long s) {
     c_.psiq = psiq_buf_[s % 3];
     c_.psiq_old = psiq_buf_[(s + 2) % 3];
@@ -593,6 +599,15 @@ class Engine : public EngineBase {
     c_.psi = psi_buf_[s % 2];
     c_.psi_old = psi_buf_[(s + 1) % 2];
     c_.psi_new = psi_buf_[(s + 1) % 2];
+    // grad rho (the FP32 form has one buffer and no next)
+    T* const* rd = rd_buf_[kStateCopy<T> ? 0 : s % 2];
+    c_.rdx = rd[0]; c_.rdy = rd[1]; c_.rdz = rd[2];
+    if constexpr (!kStateCopy<T>) {
+      T* const* rn = rd_buf_[(s + 1) % 2];
+      c_.rdnx = rn[0]; c_.rdny = rn[1]; c_.rdnz = rn[2];
+    } else {
+      c_.rdnx = c_.rdny = c_.rdnz = nullptr;
+    }
   }
 
   void use_tma() {
@@ -653,14 +668,17 @@ class Engine : public EngineBase {
       c_.psiq_t = next();
       c_.rhoq_t = next();
     }
-    set_phase(0);
     c_.divvq = next(); c_.Sx = next(); c_.Sy = next(); c_.Sz = next();
     c_.vx = next(); c_.vy = next(); c_.vz = next(); c_.divv = next(); c_.p = next();
     c_.df = next(); c_.lap = next();
-    c_.rdx = next(); c_.rdy = next(); c_.rdz = next(); c_.ldx = next(); c_.ldy = next(); c_.ldz = next();
+    for (auto& b : rd_buf_[0]) b = next();
+    if constexpr (!kStateCopy<T>)
+      for (auto& b : rd_buf_[1]) b = next();
+    c_.ldx = next(); c_.ldy = next(); c_.ldz = next();
     c_.sh = next(); c_.dtpsi = next(); c_.tmp = next();
     if constexpr (kStateCopy<T>) c_.tmp64 = dnext();
     else c_.tmp64 = reinterpret_cast<double*>(c_.tmp);
+    set_phase(0);
     // every field inside its slab (the counts above are the slabs' sizes)
     layout_ok_ = f == static_cast<T*>(slab_) + size_t(kFields) * n_ && dfp == dslab_ + size_t(kDFields) * n_;
   }
@@ -743,7 +761,7 @@ class Engine : public EngineBase {
   int* nloop_dev_ = nullptr;
   double* partial_ = nullptr;
   cudaStream_t stream2_ = nullptr;
-  cudaEvent_t fork_ev_[10] = {};
+  cudaEvent_t fork_ev_[12] = {};
   int* tma_err_ = nullptr;
   int sms_ = 148;
   void* host_stage_ = nullptr;
@@ -757,6 +775,7 @@ class Engine : public EngineBase {
   double* psiq_buf_[3] = {};
   T* nq_buf_[2] = {};
   double* psi_buf_[2] = {};
+  T* rd_buf_[2][3] = {};   // grad rho (x, y, z); the second set in the FP64 form only
   int graph_kernels_ = 0;
   long nloop_ = 0;
 };

@@ -57,6 +57,10 @@ struct StepCtx {
   // real fields in the storage type
   T *vx, *vy, *vz, *divv, *p, *df, *lap;
   T *rdx, *rdy, *rdz, *ldx, *ldy, *ldz, *sh, *dtpsi, *tmp;
+  // FP64 form: grad rho for the next step, computed from the new rho^ with
+  // rho itself (rdx, rdy, rdz and these rotate through two buffers); the FP32
+  // form transforms grad rho from its float copy of rho^ at the step start
+  T *rdnx, *rdny, *rdnz;
 };
 
 // The FP32 form keeps separate float copies of psi^ and rho^.
@@ -731,7 +735,8 @@ cudaError_t zpass(const Geom& g, int kind, Tables<T> tb, T* src, T* dst, cudaStr
 }
 
 // psi = iCT(psiq) (quasi.cpp:1963-1965) and grad psi (quasi.cpp:1120-1186) in
-// double, in 9 axis passes instead of 12.  Each transform is separable and
+// double, in 9 axis passes instead of 12; with rho^ in place of psi^, rho =
+// iCT(rho^) (quasi.cpp:1266-1268) and grad rho (quasi.cpp:1188-1232) the same way.  Each transform is separable and
 // a multiplier or shift along one axis commutes with the passes along the
 // others, so psi, grad_y and grad_z share the plain x pass X of psiq, and psi
 // and grad_z share its plain y pass XY:
@@ -743,7 +748,8 @@ cudaError_t zpass(const Geom& g, int kind, Tables<T> tb, T* src, T* dst, cudaStr
 // fork/join pair for the second stream (nullptr: everything on s).
 template <typename T>
 cudaError_t psi_and_grad(const StepCtx<T>& c, const AxisTables<double>& tb64, const double* psiq, double* psi,
-                         cudaStream_t s, cudaStream_t s2, const cudaEvent_t* ev) {
+                         double* gx, double* gy, double* gz, cudaStream_t s, cudaStream_t s2,
+                         const cudaEvent_t* ev) {
   const Geom g = c.g;
   const bool two = s2 && ev;
   const cudaStream_t sb = two ? s2 : s;
@@ -751,15 +757,14 @@ cudaError_t psi_and_grad(const StepCtx<T>& c, const AxisTables<double>& tb64, co
     QUASI_TRY(cudaEventRecord(ev[0], s));
     QUASI_TRY(cudaStreamWaitEvent(s2, ev[0], 0));
   }
-  QUASI_TRY(inverse3_mul(g, tb64, kiSTx, psiq, MGrad<T, 0, false>{c}, 1, 0, 0, StoreField<double>{g, c.gx}, c.gx,
-                         sb));
+  QUASI_TRY(inverse3_mul(g, tb64, kiSTx, psiq, MGrad<T, 0, false>{c}, 1, 0, 0, StoreField<double>{g, gx}, gx, sb));
   double* x = c.tmp64;
   QUASI_TRY(launch_pass<double, 0>(g, E01, tb64.t[0], LoadField<double>{g, psiq}, StoreField<double>{g, x}, s));
-  QUASI_TRY(launch_mul_y_pass<double>(g, O01, tb64.t[1], x, MGrad<T, 1, false>{c}, StoreField<double>{g, c.gy}, s));
-  QUASI_TRY(zpass<double>(g, E01, tb64.t[2], c.gy, c.gy, s));
+  QUASI_TRY(launch_mul_y_pass<double>(g, O01, tb64.t[1], x, MGrad<T, 1, false>{c}, StoreField<double>{g, gy}, s));
+  QUASI_TRY(zpass<double>(g, E01, tb64.t[2], gy, gy, s));
   QUASI_TRY(launch_pass<double, 1>(g, E01, tb64.t[1], LoadField<double>{g, x}, StoreField<double>{g, x}, s));
   QUASI_TRY(zpass<double>(g, E01, tb64.t[2], x, psi, s));
-  QUASI_TRY(zpass<double>(g, O01, tb64.t[2], x, c.gz, s, 2, c.vsz));
+  QUASI_TRY(zpass<double>(g, O01, tb64.t[2], x, gz, s, 2, c.vsz));
   if (two) {
     QUASI_TRY(cudaEventRecord(ev[1], s2));
     QUASI_TRY(cudaStreamWaitEvent(s, ev[1], 0));
@@ -773,7 +778,8 @@ cudaError_t psi_and_grad(const StepCtx<T>& c, const AxisTables<double>& tb64, co
 // second stream s2 between a fork and a join (ev[2i], ev[2i+1]; ev[6] orders
 // the second stream's stress transform after the stress kernel, ev[7] the
 // density chain after the gradients, ev[8], ev[9] the fork and join of psi
-// and grad psi at the end), so that in
+// and grad psi at the end, ev[10], ev[11] those of rho and grad rho in the
+// FP64 form), so that in
 // the captured graph one persistent pass kernel's last tiles overlap the next
 // one's first loads.  s2 == nullptr: everything on s.
 // tb64: the FP64 twiddles of the double transforms (the same tables as tb in
@@ -807,9 +813,11 @@ cudaError_t enqueue_step(const StepCtx<T>& c, const AxisTables<T>& tb, const Axi
     QUASI_TRY(inverse3_mul(g, tb, kiSTx, c.psiq_t, MGrad<T, 0, true>{c}, 1, 0, 0, st(c.ldx), c.ldx, s));
     QUASI_TRY(inverse3_mul(g, tb, kiSTy, c.psiq_t, MGrad<T, 1, true>{c}, 0, 1, 0, st(c.ldy), c.ldy, sb));
     QUASI_TRY(inverse3_mul(g, tb, kiSTz, c.psiq_t, MGrad<T, 2, true>{c}, 0, 0, 1, st(c.ldz), c.ldz, s));
-    QUASI_TRY(inverse3_mul(g, tb, kiSTx, c.rhoq_t, MGrad<T, 0, false>{c}, 1, 0, 0, st(c.rdx), c.rdx, sb));
-    QUASI_TRY(inverse3_mul(g, tb, kiSTy, c.rhoq_t, MGrad<T, 1, false>{c}, 0, 1, 0, st(c.rdy), c.rdy, s));
-    QUASI_TRY(inverse3_mul(g, tb, kiSTz, c.rhoq_t, MGrad<T, 2, false>{c}, 0, 0, 1, st(c.rdz), c.rdz, sb));
+    if constexpr (kStateCopy<T>) {   // (the FP64 form computed grad rho in the previous step)
+      QUASI_TRY(inverse3_mul(g, tb, kiSTx, c.rhoq_t, MGrad<T, 0, false>{c}, 1, 0, 0, st(c.rdx), c.rdx, sb));
+      QUASI_TRY(inverse3_mul(g, tb, kiSTy, c.rhoq_t, MGrad<T, 1, false>{c}, 0, 1, 0, st(c.rdy), c.rdy, s));
+      QUASI_TRY(inverse3_mul(g, tb, kiSTz, c.rhoq_t, MGrad<T, 2, false>{c}, 0, 0, 1, st(c.rdz), c.rdz, sb));
+    }
     // the density chain must not rewrite rho^ before the grad rho transforms
     // have read it: s waits for the second stream's share ...
     if (s2) {
@@ -823,11 +831,16 @@ cudaError_t enqueue_step(const StepCtx<T>& c, const AxisTables<T>& tb, const Axi
     QUASI_EW(rho_law_kernel<T>, c, n);
     QUASI_TRY(cudaGetLastError());
     const StRhoq sr{g, c.rhoq, c.scale, c.fx, c.fy, c.fz};
-    if constexpr (kStateCopy<T>)
+    if constexpr (kStateCopy<T>) {
       QUASI_TRY(forward3(g, tb64, kCT, LoadField<double>{g, c.rho}, c.rho, StRhoqCopy<T>{sr, c.rhoq_t}, s));
-    else
+      QUASI_TRY(inverse3(g, tb64, kiCT, LoadField<double>{g, c.rhoq}, c.rho, st64(c.rho), s));
+    } else {
+      // rho and the next step's grad rho from the new rho^, sharing passes
       QUASI_TRY(forward3(g, tb64, kCT, LoadField<double>{g, c.rho}, c.rho, sr, s));
-    QUASI_TRY(inverse3(g, tb64, kiCT, LoadField<double>{g, c.rhoq}, c.rho, st64(c.rho), s));
+      QUASI_TRY(psi_and_grad(c, tb64, c.rhoq, c.rho, reinterpret_cast<double*>(c.rdnx),
+                             reinterpret_cast<double*>(c.rdny), reinterpret_cast<double*>(c.rdnz), s, s2,
+                             ev ? ev + 10 : nullptr));
+    }
     QUASI_TRY(join(0));
 
   } else {
@@ -888,7 +901,7 @@ cudaError_t enqueue_step(const StepCtx<T>& c, const AxisTables<T>& tb, const Axi
   QUASI_TRY(cudaGetLastError());
   // psi = iCT(psiq_new) and grad psi in double for the next step (psi_old <-
   // psi by rotation)
-  QUASI_TRY(psi_and_grad(c, tb64, c.psiq_new, c.psi_new, s, s2, ev ? ev + 8 : nullptr));
+  QUASI_TRY(psi_and_grad(c, tb64, c.psiq_new, c.psi_new, c.gx, c.gy, c.gz, s, s2, ev ? ev + 8 : nullptr));
   return cudaSuccess;
 }
 
@@ -912,7 +925,12 @@ __global__ void init_state_kernel(StepCtx<T> c, size_t n) {
     c.divv[id] = T(0);
     c.divvq[id] = T(0);
     c.rhoq[id] = 0.0;
-    if constexpr (kStateCopy<T>) c.rhoq_t[id] = T(0);
+    if constexpr (kStateCopy<T>) {
+      c.rhoq_t[id] = T(0);
+    } else {   // grad rho of rho^ = 0, both rotation buffers
+      c.rdx[id] = c.rdy[id] = c.rdz[id] = T(0);
+      c.rdnx[id] = c.rdny[id] = c.rdnz[id] = T(0);
+    }
     c.rho_old[id] = 0.0;
     c.vx[id] = T(0);
     c.vy[id] = T(0);
@@ -941,7 +959,7 @@ cudaError_t enqueue_init(const StepCtx<T>& c, const AxisTables<T>& tb, const Axi
     to_storage_kernel<T><<<592, 256, 0, s>>>(c.psiq, c.psiq_t, n);
     QUASI_TRY(cudaGetLastError());
   }
-  QUASI_TRY(psi_and_grad(c, tb64, c.psiq, c.psi, s, nullptr, nullptr));
+  QUASI_TRY(psi_and_grad(c, tb64, c.psiq, c.psi, c.gx, c.gy, c.gz, s, nullptr, nullptr));
   QUASI_TRY(forward3(g, tb, kCT, LdInitN<T>{c}, c.Nq_old, StoreField<T>{g, c.Nq_old}, s));
   init_state_kernel<T><<<592, 256, 0, s>>>(c, n);
   QUASI_TRY(cudaGetLastError());
