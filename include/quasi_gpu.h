@@ -173,8 +173,11 @@ QUASI_API int quasi_diagnostics(quasi_handle* h, double out[3]);
 QUASI_API int quasi_growth_rate(quasi_handle* h, double* out);
 
 /* Exact binary checkpoint of the carried state (psiq, psiq_old, Nq_old,
- * rhoq, rho_old, v, divv, psi, nLoop).  The reference restarts from psi text
- * only (quasi.cpp:692-717); quasi_set_psi + quasi_init reproduce that. */
+ * rhoq, rho, rho_old, v, divv, divvq, p, df, psi, psi_old, grad psi, grad rho
+ * in the FP64 form, the float copies of psiq and rhoq in the FP32 form, nLoop)
+ * with a checksum; a file of another grid, variant or precision is rejected.
+ * The reference restarts from psi text only (quasi.cpp:692-717);
+ * quasi_set_psi + quasi_init reproduce that. */
 QUASI_API int quasi_save(quasi_handle* h, const char* path);
 QUASI_API int quasi_load(quasi_handle* h, const char* path);
 
