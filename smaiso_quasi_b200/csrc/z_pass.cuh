@@ -337,10 +337,13 @@ template <typename T> constexpr bool zpass_root_copy() { return sizeof(T) == 4; 
 // TMA store.  One thread issues all copies; the landing buffer of tile t is
 // refilled (tile t + 2 gridDim.x) as soon as the first stage has read it, and
 // the staging rows are rewritten only after the previous store has read them.
-template <typename T, int N, int P, int KS>
+// KIND >= 0: the transform kind fixed at compile time (the launch passes the
+// same value in `kind`), so every kind-dependent branch and sign folds away.
+template <typename T, int N, int P, int KS, int KIND = -1>
 __global__ void __launch_bounds__(256, 2)
     tma_zpass_kernel(const __grid_constant__ CUtensorMap src_map, const __grid_constant__ CUtensorMap dst_map, Geom g,
                      int kind, Tables<T> tb, int ntiles, int* err, uint32_t polls, int skip, const T* mk, int rev) {
+  if constexpr (KIND >= 0) kind = KIND;
   constexpr int NT = 256, G = P / 2, SUB = (N + 255) / 256, BN = N / SUB;
   using Z = ZTile<T, N, G, NT, SUB>;
   constexpr bool kRootCopy = zpass_root_copy<T>();
@@ -452,11 +455,12 @@ struct ZwLayout {
   static_assert(size_t(R) * N * sizeof(T) <= size_t(WB), "the staging rows overlay the warp's tile");
 };
 
-template <typename T, int N, int KS>
+template <typename T, int N, int KS, int KIND = -1>
 __global__ void __launch_bounds__(256, 2)
     tma_zpass_warp_kernel(const __grid_constant__ CUtensorMap src_map, const __grid_constant__ CUtensorMap dst_map,
                           Geom g, int kind, Tables<T> tb, int ntiles, int* err, uint32_t polls, int skip,
                           const T* mk, int rev) {
+  if constexpr (KIND >= 0) kind = KIND;
   using L = ZwLayout<T, N>;
   using Z = typename L::Z;
   constexpr int G = L::G, R = L::R, RAW = L::RAW;
@@ -551,8 +555,16 @@ cudaError_t launch_zpass_warp(const Geom& g, int kind, Tables<T> tb, const T* sr
       !MapCache::get().lookup(&dmap, dst, int(sizeof(T)), g.nx, g.ny, g.nz, 2, box))
     return cudaErrorNotSupported;
   const size_t smem = L::smem_bytes();
-  auto kern = tma_zpass_warp_kernel<T, N, KS>;
-  static int per_sm = 0;   // per instantiation
+  // the 256-long passes (the headline grid's) with the kind fixed at compile time
+  using K = decltype(&tma_zpass_warp_kernel<T, N, KS>);
+  K kern = &tma_zpass_warp_kernel<T, N, KS>;
+  if constexpr (N == 256) {
+    const K ks[4] = {&tma_zpass_warp_kernel<T, N, KS, E10>, &tma_zpass_warp_kernel<T, N, KS, E01>,
+                     &tma_zpass_warp_kernel<T, N, KS, O10>, &tma_zpass_warp_kernel<T, N, KS, O01>};
+    kern = ks[kind & 3];
+  }
+  static int per_sm_k[5] = {};   // per instantiation: the runtime-kind kernel, then one per fixed kind
+  int& per_sm = per_sm_k[N == 256 ? 1 + (kind & 3) : 0];
   if (per_sm == 0) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
@@ -586,8 +598,15 @@ cudaError_t launch_zpass_nk(const Geom& g, int kind, Tables<T> tb, const T* src,
     return cudaErrorNotSupported;
   const size_t smem = size_t(2) * P * N * sizeof(T) + ((Z::cb_bytes() + 15) / 16) * 16 + 16 +
                       (zpass_root_copy<T>() ? 3 : 2) * N * sizeof(Cx<T>);
-  auto kern = tma_zpass_kernel<T, N, P, KS>;
-  static int per_sm = 0;   // per instantiation
+  using K = decltype(&tma_zpass_kernel<T, N, P, KS>);
+  K kern = &tma_zpass_kernel<T, N, P, KS>;
+  if constexpr (N == 256) {
+    const K ks[4] = {&tma_zpass_kernel<T, N, P, KS, E10>, &tma_zpass_kernel<T, N, P, KS, E01>,
+                     &tma_zpass_kernel<T, N, P, KS, O10>, &tma_zpass_kernel<T, N, P, KS, O01>};
+    kern = ks[kind & 3];
+  }
+  static int per_sm_k[5] = {};   // per instantiation: the runtime-kind kernel, then one per fixed kind
+  int& per_sm = per_sm_k[N == 256 ? 1 + (kind & 3) : 0];
   if (per_sm == 0) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
