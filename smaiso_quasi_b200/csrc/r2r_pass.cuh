@@ -437,12 +437,15 @@ template <typename T, int N, int P> constexpr int tma_work_elems() { return ((P 
 // over the work tile and one thread stores the tile through dmap (dmap2 for
 // the dual pass's second output); the next tile's first stage waits for the
 // store to have read them.
+// KIND >= 0: the transform kind fixed at compile time (the launch passes the
+// same value in `kind`), so every kind-dependent branch and sign folds away.
 template <typename T, int N, int AXIS, int P, class Store, class Mul, class Mul2 = NoMul, bool TSTORE = false,
-          int TABS = 0>
+          int TABS = 0, int KIND = -1>
 __global__ void __launch_bounds__(tma_threads<T>(), 2)
     tma_pass_kernel(const __grid_constant__ CUtensorMap map, Geom g, int kind, Tables<T> tb, Store st, int ntiles,
                     int* err, uint32_t polls, int skip, Mul mul, int dc1, int dc2, int ks, Store st2, Mul2 mul2,
                     const __grid_constant__ CUtensorMap dmap, const __grid_constant__ CUtensorMap dmap2) {
+  if constexpr (KIND >= 0) kind = KIND;
   static_assert(!TSTORE || AXIS != 2, "TMA-stored tiles are x / y passes");
   constexpr bool kDual = !std::is_same<Mul2, NoMul>::value;
   static_assert(!TSTORE || !kDual || IsStoreField<Store>::value, "dual passes stage plain fields");
@@ -898,8 +901,30 @@ cudaError_t launch_tma_pass(const Geom& g, int kind, Tables<T> tb, const T* src,
   }
   constexpr int TABS = AXIS == 2 ? 0 : row_tables<AXIS, Mul, Mul2>(tma_smem_bytes<T, N, P>(), N);
   const size_t smem = tma_smem_bytes<T, N, P>() + size_t(TABS) * N * sizeof(double);
-  auto kern = tma_pass_kernel<T, N, AXIS, P, Store, Mul, Mul2, TSTORE, TABS>;
-  static int per_sm = 0;   // per instantiation: resident CTAs per SM
+  // x / y passes of length 256 (the headline grid's) with the kind fixed at
+  // compile time: every kind for plain passes, the inverse kinds for passes
+  // with a spectral multiplier (which are always inverse transforms)
+  using K = decltype(&tma_pass_kernel<T, N, AXIS, P, Store, Mul, Mul2, TSTORE, TABS>);
+  K kern = &tma_pass_kernel<T, N, AXIS, P, Store, Mul, Mul2, TSTORE, TABS>;
+  int slot = 0;
+  if constexpr (N == 256 && AXIS != 2) {
+    if constexpr (!Mul::kActive) {
+      const K kk[4] = {&tma_pass_kernel<T, N, AXIS, P, Store, Mul, Mul2, TSTORE, TABS, E10>,
+                       &tma_pass_kernel<T, N, AXIS, P, Store, Mul, Mul2, TSTORE, TABS, E01>,
+                       &tma_pass_kernel<T, N, AXIS, P, Store, Mul, Mul2, TSTORE, TABS, O10>,
+                       &tma_pass_kernel<T, N, AXIS, P, Store, Mul, Mul2, TSTORE, TABS, O01>};
+      kern = kk[kind & 3];
+      slot = 1 + (kind & 3);
+    } else if (kind == E01) {
+      kern = &tma_pass_kernel<T, N, AXIS, P, Store, Mul, Mul2, TSTORE, TABS, E01>;
+      slot = 1 + E01;
+    } else if (kind == O01) {
+      kern = &tma_pass_kernel<T, N, AXIS, P, Store, Mul, Mul2, TSTORE, TABS, O01>;
+      slot = 1 + O01;
+    }
+  }
+  static int per_sm_k[5] = {};   // per instantiation: resident CTAs per SM (runtime kind, then per fixed kind)
+  int& per_sm = per_sm_k[slot];
   if (per_sm == 0) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
