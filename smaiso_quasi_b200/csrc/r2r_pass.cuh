@@ -427,6 +427,9 @@ __device__ __forceinline__ void tma_issue_tile(const CUtensorMap* map, T* raw, u
 }
 
 template <typename T> constexpr int tma_threads() { return 256; }
+// Transform lengths whose TMA pass kernels take the kind as a template
+// parameter (one instantiation per kind; shorter ones take it at run time).
+template <int N> constexpr bool kFixedKind = N >= 64;
 
 template <typename T, int N, int P> constexpr int tma_work_elems() { return ((P * tile_ld(N) + 15) / 16) * 16; }
 
@@ -901,13 +904,13 @@ cudaError_t launch_tma_pass(const Geom& g, int kind, Tables<T> tb, const T* src,
   }
   constexpr int TABS = AXIS == 2 ? 0 : row_tables<AXIS, Mul, Mul2>(tma_smem_bytes<T, N, P>(), N);
   const size_t smem = tma_smem_bytes<T, N, P>() + size_t(TABS) * N * sizeof(double);
-  // x / y passes of length 256 (the headline grid's) with the kind fixed at
-  // compile time: every kind for plain passes, the inverse kinds for passes
+  // x / y passes (kFixedKind lengths) with the kind fixed at compile time:
+  // every kind for plain passes, the inverse kinds for passes
   // with a spectral multiplier (which are always inverse transforms)
   using K = decltype(&tma_pass_kernel<T, N, AXIS, P, Store, Mul, Mul2, TSTORE, TABS>);
   K kern = &tma_pass_kernel<T, N, AXIS, P, Store, Mul, Mul2, TSTORE, TABS>;
   int slot = 0;
-  if constexpr (N == 256 && AXIS != 2) {
+  if constexpr (kFixedKind<N> && AXIS != 2) {
     if constexpr (!Mul::kActive) {
       const K kk[4] = {&tma_pass_kernel<T, N, AXIS, P, Store, Mul, Mul2, TSTORE, TABS, E10>,
                        &tma_pass_kernel<T, N, AXIS, P, Store, Mul, Mul2, TSTORE, TABS, E01>,

@@ -555,16 +555,16 @@ cudaError_t launch_zpass_warp(const Geom& g, int kind, Tables<T> tb, const T* sr
       !MapCache::get().lookup(&dmap, dst, int(sizeof(T)), g.nx, g.ny, g.nz, 2, box))
     return cudaErrorNotSupported;
   const size_t smem = L::smem_bytes();
-  // the 256-long passes (the headline grid's) with the kind fixed at compile time
+  // the kind fixed at compile time (kFixedKind lengths)
   using K = decltype(&tma_zpass_warp_kernel<T, N, KS>);
   K kern = &tma_zpass_warp_kernel<T, N, KS>;
-  if constexpr (N == 256) {
+  if constexpr (kFixedKind<N>) {
     const K ks[4] = {&tma_zpass_warp_kernel<T, N, KS, E10>, &tma_zpass_warp_kernel<T, N, KS, E01>,
                      &tma_zpass_warp_kernel<T, N, KS, O10>, &tma_zpass_warp_kernel<T, N, KS, O01>};
     kern = ks[kind & 3];
   }
   static int per_sm_k[5] = {};   // per instantiation: the runtime-kind kernel, then one per fixed kind
-  int& per_sm = per_sm_k[N == 256 ? 1 + (kind & 3) : 0];
+  int& per_sm = per_sm_k[kFixedKind<N> ? 1 + (kind & 3) : 0];
   if (per_sm == 0) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
@@ -600,13 +600,13 @@ cudaError_t launch_zpass_nk(const Geom& g, int kind, Tables<T> tb, const T* src,
                       (zpass_root_copy<T>() ? 3 : 2) * N * sizeof(Cx<T>);
   using K = decltype(&tma_zpass_kernel<T, N, P, KS>);
   K kern = &tma_zpass_kernel<T, N, P, KS>;
-  if constexpr (N == 256) {
+  if constexpr (kFixedKind<N>) {
     const K ks[4] = {&tma_zpass_kernel<T, N, P, KS, E10>, &tma_zpass_kernel<T, N, P, KS, E01>,
                      &tma_zpass_kernel<T, N, P, KS, O10>, &tma_zpass_kernel<T, N, P, KS, O01>};
     kern = ks[kind & 3];
   }
   static int per_sm_k[5] = {};   // per instantiation: the runtime-kind kernel, then one per fixed kind
-  int& per_sm = per_sm_k[N == 256 ? 1 + (kind & 3) : 0];
+  int& per_sm = per_sm_k[kFixedKind<N> ? 1 + (kind & 3) : 0];
   if (per_sm == 0) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
