@@ -205,11 +205,18 @@ struct StRhoq {
   }
 };
 // The FP32 form's storer also writes the float copy that the grad rho
-// transforms read (no staging: two outputs).
+// transforms read: rho^ itself is staged and leaves by the tile's TMA store,
+// the copy by plain stores from value().
 template <typename T>
 struct StRhoqCopy {
   StRhoq r;
   T* rhoq_t;
+  __host__ __device__ double* stage_dst() const { return r.rhoq; }
+  __device__ double value(int i, int j, int k, double v) const {
+    const double x = r.value(i, j, k, v);
+    rhoq_t[lin(r.g, i, j, k)] = T(x);
+    return x;
+  }
   __device__ void operator()(int i, int j, int k, double v) const {
     const double x = r.value(i, j, k, v);
     const size_t id = lin(r.g, i, j, k);
