@@ -185,8 +185,8 @@ template <typename T, int A, bool LAP> struct MGrad {
 
 // rhoq = scale CT(rho) exp(-1.57^2 q^2 8)                     quasi.cpp:1260-1261
 // The storer of the last (x) pass of the FP64 transform of rho, the Gaussian
-// as the product of its per-axis factors (host tables in double).  The FP64
-// form stages the values for the pass's TMA store.
+// as the product of its per-axis factors (host tables in double).  The values
+// are staged for the pass's TMA store (in both forms).
 struct StRhoq {
   Geom g;
   double* rhoq;
